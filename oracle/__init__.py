@@ -1,0 +1,177 @@
+"""Test infrastructure: ctypes loaders for the two CPU checkers.
+
+* ``Oracle``    -- our own scalar C restatement of the reference's multiply hot
+                   path (oracle/fastfib_oracle.c, built by ``make -C oracle``).
+* ``Reference`` -- the unmodified reference compiled from its sources with a
+                   Linux shim (oracle/ref_harness.c, ``make -C oracle ref``).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, and only as the checker.  Numbers cross the boundary as numpy
+uint64 limb arrays (little-endian 64-bit limbs, as the reference's Big).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libfastfib_ref.so")
+REF_SRC = "/root/reference"
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_szp = ctypes.POINTER(ctypes.c_size_t)
+
+
+def build(with_reference: bool = True) -> None:
+    """Builds the oracle library, and the reference too when its sources exist."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if with_reference and os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
+
+
+def int_to_limbs(x: int) -> np.ndarray:
+    """Python int -> uint64 limbs, little-endian, normalized (zero is [0])."""
+    if x < 0:
+        raise ValueError("negative")
+    n = max(1, (x.bit_length() + 63) // 64)
+    return np.frombuffer(x.to_bytes(8 * n, "little"), dtype=np.uint64).copy()
+
+
+def limbs_to_int(a: np.ndarray) -> int:
+    return int.from_bytes(np.ascontiguousarray(a, dtype=np.uint64).tobytes(), "little")
+
+
+def _arr(a: np.ndarray):
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return a, a.ctypes.data_as(_u64p), a.size
+
+
+class _Lib:
+    prefix = ""
+
+    def __init__(self, path: str):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (make -C oracle{' ref' if 'ref' in path else ''})")
+        self.lib = ctypes.CDLL(path)
+        p = self.prefix
+        for name in ("mul", "mul_ntt"):
+            f = getattr(self.lib, f"{p}{name}")
+            f.restype = ctypes.c_void_p
+            f.argtypes = [_u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, ctypes.c_int, _szp]
+        f = getattr(self.lib, f"{p}fibonacci")
+        f.restype = ctypes.c_void_p
+        f.argtypes = [ctypes.c_uint64, _szp]
+        f = getattr(self.lib, f"{p}to_string")
+        f.restype = ctypes.c_void_p
+        f.argtypes = [_u64p, ctypes.c_size_t]
+        getattr(self.lib, f"{p}free").argtypes = [ctypes.c_void_p]
+        getattr(self.lib, f"{p}ntt_init").argtypes = [ctypes.c_size_t]
+        getattr(self.lib, f"{p}ntt_max_L").restype = ctypes.c_size_t
+        getattr(self.lib, f"{p}set_ntt_max_L").argtypes = [ctypes.c_size_t]
+
+    def _take(self, ptr, n) -> np.ndarray:
+        out = np.ctypeslib.as_array(ctypes.cast(ptr, _u64p), shape=(n,)).copy()
+        getattr(self.lib, f"{self.prefix}free")(ptr)
+        return out
+
+    def _mul(self, name, a, b, square):
+        a, pa, na = _arr(a)
+        if square:
+            b, pb, nb = a, pa, na
+        else:
+            b, pb, nb = _arr(b)
+        n = ctypes.c_size_t()
+        ptr = getattr(self.lib, f"{self.prefix}{name}")(pa, na, pb, nb, int(square), ctypes.byref(n))
+        return self._take(ptr, n.value)
+
+    def mul(self, a, b=None, square=False):
+        """big_mul / big_sqr: the threshold dispatch."""
+        return self._mul("mul", a, a if b is None else b, square or b is None)
+
+    def mul_ntt(self, a, b=None, square=False):
+        """big_mul_ntt: the NTT multiply (square when b is None)."""
+        return self._mul("mul_ntt", a, a if b is None else b, square or b is None)
+
+    def fibonacci(self, n: int) -> np.ndarray:
+        k = ctypes.c_size_t()
+        ptr = getattr(self.lib, f"{self.prefix}fibonacci")(n, ctypes.byref(k))
+        return self._take(ptr, k.value)
+
+    def to_string(self, a) -> str:
+        a, pa, na = _arr(a)
+        ptr = getattr(self.lib, f"{self.prefix}to_string")(pa, na)
+        s = ctypes.string_at(ptr).decode()
+        getattr(self.lib, f"{self.prefix}free")(ptr)
+        return s
+
+    def ntt_init(self, max_limbs: int) -> None:
+        getattr(self.lib, f"{self.prefix}ntt_init")(max_limbs)
+
+    def ntt_max_L(self) -> int:
+        return getattr(self.lib, f"{self.prefix}ntt_max_L")()
+
+    def set_ntt_max_L(self, L: int) -> None:
+        getattr(self.lib, f"{self.prefix}set_ntt_max_L")(L)
+
+
+class FoPlan(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("lg", ctypes.c_uint32), ("r3", ctypes.c_uint32),
+                ("split", ctypes.c_uint32), ("L", ctypes.c_uint64), ("conv", ctypes.c_uint64),
+                ("ca", ctypes.c_uint64), ("cb", ctypes.c_uint64), ("ka", ctypes.c_uint64),
+                ("kb", ctypes.c_uint64), ("Lbig", ctypes.c_uint64)]
+
+
+class Oracle(_Lib):
+    """Our scalar C restatement (oracle/fastfib_oracle.c)."""
+    prefix = "fo_"
+
+    def __init__(self, path: str = ORACLE_SO):
+        super().__init__(path)
+        self.lib.fo_ntt_plan.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(FoPlan)]
+        self.lib.fo_ntt_plan.restype = ctypes.c_int
+        self.lib.fo_fingerprint.argtypes = [_u64p, ctypes.c_size_t, _u64p]
+        self.lib.fo_mul_ntt_forced.restype = ctypes.c_void_p
+        self.lib.fo_mul_ntt_forced.argtypes = [_u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, ctypes.c_int,
+                                               ctypes.c_uint32, ctypes.c_uint64, _szp]
+
+    def plan(self, bits_a: int, bits_b: int, square: bool = False) -> FoPlan:
+        p = FoPlan()
+        self.lib.fo_ntt_plan(bits_a, bits_b, int(square), ctypes.byref(p))
+        return p
+
+    def mul_ntt_forced(self, a, b, width: int, L: int, square=False):
+        a, pa, na = _arr(a)
+        b, pb, nb = (a, pa, na) if square else _arr(b)
+        n = ctypes.c_size_t()
+        ptr = self.lib.fo_mul_ntt_forced(pa, na, pb, nb, int(square), width, L, ctypes.byref(n))
+        return self._take(ptr, n.value)
+
+    def fingerprint(self, a) -> tuple:
+        a, pa, na = _arr(a)
+        out = (ctypes.c_uint64 * 6)()
+        self.lib.fo_fingerprint(pa, na, out)
+        return tuple(int(v) for v in out)
+
+
+class Reference(_Lib):
+    """The unmodified reference built from its sources (oracle/_ref)."""
+    prefix = "ffref_"
+
+    def __init__(self, path: str = REF_SO):
+        super().__init__(path)
+        self.lib.ffref_seconds.restype = ctypes.c_double
+        self.lib.ffref_cpus.restype = ctypes.c_int
+
+    def seconds(self) -> float:
+        return self.lib.ffref_seconds()
+
+    def cpus(self) -> int:
+        return self.lib.ffref_cpus()
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)
