@@ -1,0 +1,218 @@
+"""fastfib_b200: the reference's multiply hot path on a B200.
+
+A ctypes mirror of the two C interfaces of ``libfastfib_b200.so``:
+
+* the reference's own surface (include/fastfib.h): ``big_mul``, ``big_sqr``,
+  ``big_mul_ntt``, ``fibonacci``, ``big_to_string``, ``ntt_init`` and the
+  transform cap ``g_ntt_max_L``, with the same names and meaning;
+* the thin GPU ABI (include/ffg.h): plans, device-pointer products, the
+  device fast-doubling chain.
+
+Numbers cross as numpy uint64 limb arrays (little-endian 64-bit limbs, the
+reference's Big).  There is no CPU fallback: if the library or a GPU is
+missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libfastfib_b200.so")
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_szp = ctypes.POINTER(ctypes.c_size_t)
+
+
+class Big(ctypes.Structure):
+    """The reference's Big (src/common.h:29-33)."""
+    _fields_ = [("d", _u64p), ("n", ctypes.c_size_t)]
+
+
+class Plan(ctypes.Structure):
+    """ffg_plan (include/ffg.h)."""
+    _fields_ = [("width", ctypes.c_uint32), ("lg", ctypes.c_uint32), ("r3", ctypes.c_uint32),
+                ("split", ctypes.c_uint32), ("L", ctypes.c_uint64), ("conv", ctypes.c_uint64),
+                ("ca", ctypes.c_uint64), ("cb", ctypes.c_uint64), ("ka", ctypes.c_uint64),
+                ("kb", ctypes.c_uint64), ("Lbig", ctypes.c_uint64), ("kernel", ctypes.c_uint32),
+                ("row_lg", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+class FfgError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libfastfib_b200.so (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FfgError(f"{LIB_PATH} is not built: run python -m fastfib_b200.build")
+    L = ctypes.CDLL(LIB_PATH)
+    L.ffg_init.argtypes = [ctypes.c_size_t]
+    L.ffg_ntt_max_L.restype = ctypes.c_size_t
+    L.ffg_set_ntt_max_L.argtypes = [ctypes.c_size_t]
+    L.ffg_plan_select.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(Plan)]
+    L.ffg_mul_host.argtypes = [_u64p, _szp, _u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, ctypes.c_int]
+    L.ffg_mul_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64,
+                                 ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int,
+                                 ctypes.c_void_p]
+    L.ffg_fib_chain.argtypes = [ctypes.c_uint64, ctypes.c_int, _u64p, ctypes.c_size_t, _u64p,
+                                ctypes.c_size_t, ctypes.POINTER(_u64p), _szp]
+    L.ffg_last_chain_ms.restype = ctypes.c_double
+    L.ffg_last_error.restype = ctypes.c_char_p
+    L.ffg_free.argtypes = [ctypes.c_void_p]
+    for name in ("big_mul", "big_mul_ntt", "big_mul_toom3"):
+        getattr(L, name).restype = Big
+        getattr(L, name).argtypes = [ctypes.POINTER(Big), ctypes.POINTER(Big)]
+    L.big_sqr.restype = Big
+    L.big_sqr.argtypes = [ctypes.POINTER(Big)]
+    L.fibonacci.restype = Big
+    L.fibonacci.argtypes = [ctypes.c_uint64]
+    L.big_to_string.restype = ctypes.c_void_p
+    L.big_to_string.argtypes = [ctypes.POINTER(Big)]
+    L.big_free.argtypes = [ctypes.POINTER(Big)]
+    L.ntt_init.argtypes = [ctypes.c_size_t]
+    L.plat_seconds.restype = ctypes.c_double
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc:
+        raise FfgError(f"ffg error {rc}: {lib().ffg_last_error().decode()}")
+
+
+def _arr(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    if a.size == 0:
+        a = np.zeros(1, dtype=np.uint64)
+    return a
+
+
+def _view(a: np.ndarray) -> Big:
+    n = a.size
+    while n > 1 and a[n - 1] == 0:
+        n -= 1
+    return Big(a.ctypes.data_as(_u64p), n)
+
+
+def _take(b: Big) -> np.ndarray:
+    out = np.ctypeslib.as_array(b.d, shape=(b.n,)).copy()
+    lib().big_free(ctypes.byref(b))
+    return out
+
+
+def int_to_limbs(x: int) -> np.ndarray:
+    n = max(1, (x.bit_length() + 63) // 64)
+    return np.frombuffer(x.to_bytes(8 * n, "little"), dtype=np.uint64).copy()
+
+
+def limbs_to_int(a: np.ndarray) -> int:
+    return int.from_bytes(np.ascontiguousarray(a, dtype=np.uint64).tobytes(), "little")
+
+
+# ------------------------------------------------------------ the C surface
+
+def g_ntt_max_L() -> int:
+    return ctypes.c_size_t.in_dll(lib(), "g_ntt_max_L").value
+
+
+def set_g_ntt_max_L(L: int) -> None:
+    """Overrides the transform cap, as tests/nttfuzz.c:33-39 does."""
+    ctypes.c_size_t.in_dll(lib(), "g_ntt_max_L").value = L
+
+
+def ntt_init(max_limbs: int) -> None:
+    lib().ntt_init(max_limbs)
+
+
+def big_mul(a, b) -> np.ndarray:
+    a, b = _arr(a), _arr(b)
+    A, B = _view(a), _view(b)
+    return _take(lib().big_mul(ctypes.byref(A), ctypes.byref(B)))
+
+
+def big_sqr(a) -> np.ndarray:
+    a = _arr(a)
+    A = _view(a)
+    return _take(lib().big_sqr(ctypes.byref(A)))
+
+
+def big_mul_ntt(a, b=None) -> np.ndarray:
+    """big_mul_ntt; b None squares (the reference passes a == b)."""
+    a = _arr(a)
+    A = _view(a)
+    if b is None:
+        return _take(lib().big_mul_ntt(ctypes.byref(A), ctypes.byref(A)))
+    b = _arr(b)
+    B = _view(b)
+    return _take(lib().big_mul_ntt(ctypes.byref(A), ctypes.byref(B)))
+
+
+def fibonacci(n: int) -> np.ndarray:
+    return _take(lib().fibonacci(n))
+
+
+def big_to_string(a) -> str:
+    a = _arr(a)
+    A = _view(a)
+    p = lib().big_to_string(ctypes.byref(A))
+    s = ctypes.string_at(p).decode()
+    ctypes.CDLL(None).free(ctypes.c_void_p(p))
+    return s
+
+
+# ------------------------------------------------------------------ the GPU ABI
+
+def init(max_limbs: int) -> None:
+    _check(lib().ffg_init(max_limbs))
+
+
+def plan(bits_a: int, bits_b: int, square: bool = False) -> dict:
+    p = Plan()
+    _check(lib().ffg_plan_select(bits_a, bits_b, int(square), ctypes.byref(p)))
+    return p.as_dict()
+
+
+def mul(a, b=None) -> np.ndarray:
+    """ffg_mul_host: the NTT product on the GPU (b None squares)."""
+    a = _arr(a)
+    sq = b is None
+    b = a if sq else _arr(b)
+    out = np.zeros(a.size + b.size + 1, dtype=np.uint64)
+    n = ctypes.c_size_t()
+    _check(lib().ffg_mul_host(out.ctypes.data_as(_u64p), ctypes.byref(n), a.ctypes.data_as(_u64p), a.size,
+                              b.ctypes.data_as(_u64p), b.size, int(sq)))
+    return out[: n.value].copy()
+
+
+def mul_device(out_ptr: int, a_ptr: int, na: int, bits_a: int, b_ptr: int, nb: int, bits_b: int,
+               square: bool = False, stream: int = 0) -> None:
+    """ffg_mul_device on device pointers (e.g. torch tensors' data_ptr())."""
+    _check(lib().ffg_mul_device(out_ptr, a_ptr, na, bits_a, b_ptr if not square else a_ptr, nb, bits_b,
+                                int(square), stream or None))
+
+
+def fib_chain(n: int, i0: int, fkm1, fk) -> np.ndarray:
+    fkm1, fk = _arr(fkm1), _arr(fk)
+    out = _u64p()
+    nout = ctypes.c_size_t()
+    _check(lib().ffg_fib_chain(n, i0, fkm1.ctypes.data_as(_u64p), fkm1.size, fk.ctypes.data_as(_u64p),
+                               fk.size, ctypes.byref(out), ctypes.byref(nout)))
+    r = np.ctypeslib.as_array(out, shape=(nout.value,)).copy()
+    lib().ffg_free(out)
+    return r
+
+
+def last_chain_ms() -> float:
+    return lib().ffg_last_chain_ms()

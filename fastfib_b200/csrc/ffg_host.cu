@@ -1,0 +1,638 @@
+// Host side of the B200 layer: device tables, a block arena, the product
+// plan (the reference's width / length choice plus the GPU geometry), the
+// multiply orchestration, the device fast-doubling chain, and the C ABI
+// declared in include/ffg.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ffg.h"
+#include "ffg_internal.h"
+
+namespace ffg {
+
+typedef unsigned __int128 u128h;
+
+static const uint32_t kP[3] = {2113929217u, 2013265921u, 1811939329u}; // src/ntt_arith.c:48-52
+static const uint32_t kG[3] = {5u, 31u, 13u};
+static const int kMaxLg = 25;                                           // NTT_MAX_LG, src/common.h:46-48
+static const uint32_t kSmallMaxL = 4096;  // one-CTA transform up to this length for a single product
+static const int kR3TabLg = 13;           // radix-3 tables cover R = 3 2^n, n < 13
+
+// ------------------------------------------------------------ host modmath
+
+static uint32_t powmod(uint32_t a, uint64_t e, uint32_t p) {
+    uint64_t r = 1, x = a % p;
+    for (; e; e >>= 1, x = x * x % p)
+        if (e & 1) r = r * x % p;
+    return (uint32_t)r;
+}
+static uint32_t inv_mod(uint32_t a, uint32_t p) { return powmod(a, p - 2, p); }
+static uint32_t shoup_q(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)w << 32) / p); }
+static uint32_t to_mont(uint32_t x, uint32_t p) { return (uint32_t)(((uint64_t)x << 32) % p); }
+static uint32_t mulm(uint32_t a, uint32_t b, uint32_t p) { return (uint32_t)((uint64_t)a * b % p); }
+
+GarnerConst garner_const() {
+    GarnerConst K;
+    for (int i = 0; i < 3; i++) K.p[i] = kP[i];
+    K.i12 = inv_mod(kP[0] % kP[1], kP[1]);
+    K.i12s = shoup_q(K.i12, kP[1]);
+    K.i13 = inv_mod(kP[0] % kP[2], kP[2]);
+    K.i13s = shoup_q(K.i13, kP[2]);
+    K.i23 = inv_mod(kP[1] % kP[2], kP[2]);
+    K.i23s = shoup_q(K.i23, kP[2]);
+    K.p12 = (uint64_t)kP[0] * kP[1];
+    return K;
+}
+
+// ------------------------------------------------------------------ context
+
+struct Block {
+    char *ptr;
+    size_t cap, used;
+};
+
+struct Ctx {
+    bool ready = false;
+    cudaStream_t stream = nullptr;
+    Primes3 P3{};
+    void *tables = nullptr;
+    std::vector<Block> blocks;
+    size_t max_L = 0;
+    std::string err;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double chain_ms = 0;
+};
+
+static Ctx g;
+static std::recursive_mutex g_mu;
+
+static int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g.err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                     \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess) return fail(FFG_E_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                      \
+    } while (0)
+
+// Device tables for the three primes (see PrimeDev).
+static int build_tables() {
+    const size_t nrt = (size_t)1 << FFG_LINE_LG, nr3 = (size_t)1 << kR3TabLg;
+    const size_t ntwh = (size_t)(FFG_M / FFG_TW_LO);
+    const size_t per = nrt * 2 * sizeof(uint2) + nr3 * 2 * sizeof(uint4) + (FFG_TW_LO + ntwh) * sizeof(uint32_t);
+    std::vector<char> host(per * 3);
+    CK(cudaMalloc(&g.tables, per * 3));
+    for (int k = 0; k < 3; k++) {
+        const uint32_t p = kP[k], gen = kG[k];
+        char *hb = host.data() + per * k;
+        char *db = (char *)g.tables + per * k;
+        uint2 *rt = (uint2 *)hb, *irt = rt + nrt;
+        uint4 *r3f = (uint4 *)(irt + nrt), *r3i = r3f + nr3;
+        uint32_t *twl = (uint32_t *)(r3i + nr3), *twh = twl + FFG_TW_LO;
+        rt[0] = irt[0] = make_uint2(0, 0);
+        for (size_t h = 1; h < nrt; h <<= 1) {
+            uint32_t w = powmod(gen, (p - 1) / (2 * h), p), wi = inv_mod(w, p);
+            uint32_t c = 1, ci = 1;
+            for (size_t i = 0; i < h; i++) {
+                rt[h + i] = make_uint2(c, shoup_q(c, p));
+                irt[h + i] = make_uint2(ci, shoup_q(ci, p));
+                c = mulm(c, w, p);
+                ci = mulm(ci, wi, p);
+            }
+        }
+        r3f[0] = r3i[0] = make_uint4(0, 0, 0, 0);
+        for (int n = 0; n < kR3TabLg; n++) {
+            const uint64_t B = (uint64_t)1 << n, R = 3 * B;
+            uint32_t w = powmod(gen, (p - 1) / R, p), wi = inv_mod(w, p);
+            uint32_t c = 1, ci = 1;
+            for (uint64_t j = 0; j < B; j++) {
+                uint32_t c2 = mulm(c, c, p), ci2 = mulm(ci, ci, p);
+                r3f[B + j] = make_uint4(c, shoup_q(c, p), c2, shoup_q(c2, p));
+                r3i[B + j] = make_uint4(ci, shoup_q(ci, p), ci2, shoup_q(ci2, p));
+                c = mulm(c, w, p);
+                ci = mulm(ci, wi, p);
+            }
+        }
+        const uint32_t wM = powmod(gen, (p - 1) / FFG_M, p), wMh = powmod(wM, FFG_TW_LO, p);
+        uint32_t c = 1;
+        for (uint32_t e = 0; e < FFG_TW_LO; e++, c = mulm(c, wM, p)) twl[e] = to_mont(c, p);
+        c = 1;
+        for (size_t e = 0; e < ntwh; e++, c = mulm(c, wMh, p)) twh[e] = to_mont(c, p);
+
+        PrimeDev &P = g.P3.pr[k];
+        P.p = p;
+        uint32_t inv = p; // p^-1 mod 2^32 by Newton (p odd): 3 -> 6 -> 12 -> 24 -> 48 bits
+        for (int it = 0; it < 4; it++) inv *= 2 - p * inv;
+        P.pinv = inv;
+        P.w3 = powmod(gen, (p - 1) / 3, p);
+        P.w3s = shoup_q(P.w3, p);
+        P.v3 = inv_mod(P.w3, p);
+        P.v3s = shoup_q(P.v3, p);
+        P.c32 = (uint32_t)((1ull << 32) % p);
+        P.c32s = shoup_q(P.c32, p);
+        P.rt = (const uint2 *)db;
+        P.irt = P.rt + nrt;
+        P.r3f = (const uint4 *)(P.irt + nrt);
+        P.r3i = P.r3f + nr3;
+        P.twl = (const uint32_t *)(P.r3i + nr3);
+        P.twh = P.twl + FFG_TW_LO;
+    }
+    CK(cudaMemcpy(g.tables, host.data(), per * 3, cudaMemcpyHostToDevice));
+    return FFG_OK;
+}
+
+static int ensure_ready() {
+    if (g.ready) return FFG_OK;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(FFG_E_NODEV, "no CUDA device");
+    CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&g.ev0));
+    CK(cudaEventCreate(&g.ev1));
+    int rc = build_tables();
+    if (rc) return rc;
+    g.ready = true;
+    return FFG_OK;
+}
+
+// -------------------------------------------------------------------- arena
+
+// Bump allocation out of a list of device blocks; blocks are never moved
+// while work may be in flight, and reset() (after a synchronize) recycles them.
+static void arena_reset() {
+    for (auto &b : g.blocks) b.used = 0;
+}
+
+static void *arena_alloc(size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    for (auto &b : g.blocks)
+        if (b.cap - b.used >= bytes) {
+            void *p = b.ptr + b.used;
+            b.used += bytes;
+            return p;
+        }
+    size_t last = g.blocks.empty() ? 0 : g.blocks.back().cap;
+    size_t cap = std::max(bytes, std::max((size_t)64 << 20, 2 * last));
+    char *p = nullptr;
+    if (cudaMalloc(&p, cap) != cudaSuccess) {
+        cudaGetLastError();
+        cap = bytes;
+        if (cudaMalloc(&p, cap) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+    }
+    g.blocks.push_back({p, cap, bytes});
+    return p;
+}
+
+#define ALLOC(var, type, count)                                                                        \
+    type *var = (type *)arena_alloc((size_t)(count) * sizeof(type));                                   \
+    if (!var) return fail(FFG_E_NOMEM, "device arena: out of memory (%zu bytes)", (size_t)(count) * sizeof(type));
+
+// --------------------------------------------------------------------- plan
+
+// ntt_width_ok (src/mul_ntt.c:55-59)
+static bool width_ok(uint64_t bits_a, uint64_t bits_b, unsigned w) {
+    const u128h M = (u128h)kP[0] * kP[1] * kP[2];
+    uint64_t ca = (bits_a + w - 1) / w, cb = (bits_b + w - 1) / w;
+    return ((u128h)(ca < cb ? ca : cb) << (2 * w)) < M;
+}
+
+// ntt_length (src/mul_ntt.c:78-93)
+static uint64_t ntt_length(uint64_t conv, uint32_t *lg_out, uint32_t *r3_out) {
+    uint64_t L = 16;
+    uint32_t lg = 4, r3 = 0;
+    while (L < conv) {
+        L <<= 1;
+        lg++;
+    }
+    if (L / 4 * 3 >= conv && L / 4 >= 16) {
+        L = L / 4 * 3;
+        lg -= 2;
+        r3 = 1;
+    }
+    *lg_out = lg;
+    *r3_out = r3;
+    return L;
+}
+
+static void gpu_geometry(ffg_plan *pl) {
+    if (pl->L <= kSmallMaxL) {
+        pl->kernel = 0;
+        pl->row_lg = 0;
+        return;
+    }
+    int c = (int)pl->lg - 7;
+    c = c < 8 ? 8 : (c > 13 ? 13 : c);
+    pl->kernel = 1;
+    pl->row_lg = (uint32_t)c;
+}
+
+static int plan_select(uint64_t bits_a, uint64_t bits_b, int square, ffg_plan *pl) {
+    memset(pl, 0, sizeof *pl);
+    uint64_t L = 0;
+    for (unsigned w = 32; w <= 35; w++) {
+        if (!width_ok(bits_a, bits_b, w)) break;
+        uint64_t ca = (bits_a + w - 1) / w, cb = (bits_b + w - 1) / w;
+        uint32_t lg, r3;
+        uint64_t Lw = ntt_length(ca + cb - 1, &lg, &r3);
+        if (L == 0 || Lw < L) {
+            L = Lw;
+            pl->L = Lw, pl->lg = lg, pl->r3 = r3, pl->width = w;
+            pl->ca = ca, pl->cb = cb, pl->conv = ca + cb - 1;
+        }
+    }
+    (void)square;
+    if (L == 0 || L > g.max_L) {
+        pl->split = 1;
+        return fail(FFG_E_RANGE, "product of %llu x %llu bits needs the split multiply (L=%llu > cap %zu)",
+                    (unsigned long long)bits_a, (unsigned long long)bits_b, (unsigned long long)L, g.max_L);
+    }
+    gpu_geometry(pl);
+    return FFG_OK;
+}
+
+// 2^32 / L mod p as Shoup pairs (undoes the pointwise 2^-32 and the inverse's L).
+static void scale_consts(uint64_t L, uint32_t *scl, uint32_t *scls) {
+    for (int k = 0; k < 3; k++) {
+        uint32_t p = kP[k];
+        uint32_t v = mulm((uint32_t)((1ull << 32) % p), inv_mod((uint32_t)(L % p), p), p);
+        scl[k] = v;
+        scls[k] = shoup_q(v, p);
+    }
+}
+
+// ---------------------------------------------------------------- multiply
+
+struct Prod {
+    const uint64_t *a, *b;
+    uint64_t na, nb, bits_a, bits_b;
+    uint64_t *out;   // na + nb + 1 limbs
+    int64_t add;     // small constant added to the product
+};
+
+// Products that share one plan (same width, length, squareness), run as one
+// batch of transforms, then one CRT each.
+static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool square, cudaStream_t st) {
+    const uint64_t L = pl.L;
+    uint32_t scl[3], scls[3];
+    scale_consts(L, scl, scls);
+    std::vector<uint32_t *> ya(count), yb(count);
+    for (int i = 0; i < count; i++) {
+        ya[i] = (uint32_t *)arena_alloc(3 * L * sizeof(uint32_t));
+        yb[i] = square ? nullptr : (uint32_t *)arena_alloc(3 * L * sizeof(uint32_t));
+        if (!ya[i] || (!square && !yb[i])) return fail(FFG_E_NOMEM, "device arena: residues of L=%llu",
+                                                      (unsigned long long)L);
+    }
+    const uint32_t w = pl.width;
+    cudaError_t e = cudaSuccess;
+    if (pl.kernel == 0) {
+        for (int i = 0; i < count; i++) {
+            ConvJob J{};
+            J.a = pr[i].a, J.b = square ? pr[i].a : pr[i].b;
+            J.na = pr[i].na, J.nb = square ? pr[i].na : pr[i].nb;
+            J.ca = (pr[i].bits_a + w - 1) / w;
+            J.cb = square ? J.ca : (pr[i].bits_b + w - 1) / w;
+            J.y = ya[i];
+            J.y_stride = L;
+            J.L_words = (uint32_t)L;
+            J.n = pl.lg, J.r3 = pl.r3, J.width = w, J.square = square;
+            J.conv = (uint32_t)(J.ca + J.cb - 1);
+            memcpy(J.scl, scl, sizeof scl);
+            memcpy(J.scls, scls, sizeof scls);
+            ALLOC(dj, ConvJob, 1);
+            CK(cudaMemcpyAsync(dj, &J, sizeof J, cudaMemcpyHostToDevice, st));
+            e = launch_conv_small(g.P3, dj, 1, (uint32_t)L, !square, st);
+            if (e) return fail(FFG_E_CUDA, "conv_small: %s", cudaGetErrorString(e));
+        }
+    } else {
+        FourStep G{};
+        G.L = L;
+        G.c = pl.row_lg;
+        G.rn = pl.lg - G.c;
+        G.r3 = pl.r3;
+        G.R = (pl.r3 ? 3u : 1u) << G.rn;
+        uint32_t wc = 32768u / G.R;
+        wc = wc < 8 ? 8 : (wc > 64 ? 64 : wc);
+        while (wc & (wc - 1)) wc &= wc - 1;
+        if (wc > (1u << G.c)) wc = 1u << G.c;
+        G.wc = wc;
+        G.col_stride = line_stride(G.R);
+        G.square = square;
+        G.mstep = FFG_M / L;
+        memcpy(G.scl, scl, sizeof scl);
+        memcpy(G.scls, scls, sizeof scls);
+        std::vector<FSJob> jobs(count);
+        for (int i = 0; i < count; i++) {
+            FSJob &J = jobs[i];
+            J.a = pr[i].a, J.b = square ? pr[i].a : pr[i].b;
+            J.na = pr[i].na, J.nb = square ? pr[i].na : pr[i].nb;
+            J.ca = (pr[i].bits_a + w - 1) / w;
+            J.cb = square ? J.ca : (pr[i].bits_b + w - 1) / w;
+            J.ya = ya[i], J.yb = yb[i];
+            J.width = w;
+        }
+        ALLOC(dj, FSJob, count);
+        CK(cudaMemcpyAsync(dj, jobs.data(), count * sizeof(FSJob), cudaMemcpyHostToDevice, st));
+        e = launch_four_step(g.P3, G, dj, (uint32_t)count, st);
+        if (e) return fail(FFG_E_CUDA, "four_step: %s", cudaGetErrorString(e));
+    }
+    for (int i = 0; i < count; i++) {
+        CrtJob C{};
+        C.y = ya[i];
+        C.y_stride = L;
+        uint64_t ca = (pr[i].bits_a + w - 1) / w, cb = square ? ca : (pr[i].bits_b + w - 1) / w;
+        C.conv = ca + cb - 1;
+        C.out = pr[i].out;
+        C.nlimbs = pr[i].na + (square ? pr[i].na : pr[i].nb) + 1;
+        C.width = w;
+        C.nchunks = (uint32_t)((C.nlimbs + w - 1) / w);
+        C.add = pr[i].add;
+        uint32_t ncta = (C.nchunks + FFG_CRT_THREADS - 1) / FFG_CRT_THREADS;
+        C.pref = (StepFn *)arena_alloc((size_t)C.nchunks * sizeof(StepFn));
+        C.cta_fn = (StepFn *)arena_alloc((size_t)ncta * sizeof(StepFn));
+        C.cta_in = (__int128 *)arena_alloc((size_t)ncta * sizeof(__int128));
+        if (!C.pref || !C.cta_fn || !C.cta_in) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
+        e = launch_crt(g.P3, C, st);
+        if (e) return fail(FFG_E_CUDA, "crt: %s", cudaGetErrorString(e));
+    }
+    return FFG_OK;
+}
+
+// One product on device limbs (plan from the bit lengths).
+static int mul_one(const Prod &p, bool square, cudaStream_t st) {
+    ffg_plan pl;
+    int rc = plan_select(p.bits_a, square ? p.bits_a : p.bits_b, square, &pl);
+    if (rc) return rc;
+    return run_products(&p, 1, pl, square, st);
+}
+
+static uint64_t bits_of(const uint64_t *a, size_t n) {
+    while (n > 0 && a[n - 1] == 0) n--;
+    if (n == 0) return 0;
+    return 64 * (n - 1) + (64 - (uint64_t)__builtin_clzll(a[n - 1]));
+}
+
+// -------------------------------------------------------- fast doubling
+
+static const long double kLog2Phi = 0.6942419136306174017387902668985552L;
+static const long double kLog2Sqrt5 = 1.1609640474436811739351597147446950L;
+
+// Bit length of F(m) (m >= 2): floor(m log2(phi) - log2(sqrt 5)) + 1, since
+// F(m) = round(phi^m / sqrt 5).  When the value sits too close to an integer
+// for long double to decide, one more bit is returned (a safe upper bound).
+static uint64_t fib_bits(uint64_t m) {
+    long double x = (long double)m * kLog2Phi - kLog2Sqrt5, f = floorl(x);
+    uint64_t b = (uint64_t)f + 1;
+    if (x - f < 1e-7L || f + 1 - x < 1e-7L) b++;
+    return b;
+}
+// Bit length of the Lucas number L(m) = round(phi^m) (m >= 2), same guard.
+static uint64_t lucas_bits(uint64_t m) {
+    long double x = (long double)m * kLog2Phi, f = floorl(x);
+    uint64_t b = (uint64_t)f + 1;
+    if (x - f < 1e-7L || f + 1 - x < 1e-7L) b++;
+    return b;
+}
+
+static int lin(const uint64_t *s1, uint64_t n1, const uint64_t *s2, uint64_t n2, uint64_t len, int nout,
+               uint64_t *o0, int a0, int b0, int64_t g0, uint64_t *o1, int a1, int b1, int64_t g1, cudaStream_t st) {
+    LinJob J{};
+    J.s1 = s1, J.s2 = s2, J.n1 = n1, J.n2 = n2, J.len = len;
+    J.out[0] = o0, J.out[1] = o1;
+    J.alpha[0] = a0, J.beta[0] = b0, J.gamma[0] = g0;
+    J.alpha[1] = a1, J.beta[1] = b1, J.gamma[1] = g1;
+    J.nout = (uint32_t)nout;
+    J.nchunks = (uint32_t)((len + FFG_LIN_K - 1) / FFG_LIN_K);
+    uint32_t ncta = (J.nchunks + FFG_LIN_THREADS - 1) / FFG_LIN_THREADS;
+    J.pref = (StepFn *)arena_alloc(2 * (size_t)J.nchunks * sizeof(StepFn));
+    J.cta_fn = (StepFn *)arena_alloc(2 * (size_t)ncta * sizeof(StepFn));
+    J.cta_in = (__int128 *)arena_alloc(2 * (size_t)ncta * sizeof(__int128));
+    if (!J.pref || !J.cta_fn || !J.cta_in) return fail(FFG_E_NOMEM, "device arena: linear pass scratch");
+    cudaError_t e = launch_lin(J, st);
+    if (e) return fail(FFG_E_CUDA, "linear pass: %s", cudaGetErrorString(e));
+    return FFG_OK;
+}
+
+static int fib_chain(uint64_t n, int i0, const uint64_t *hkm1, size_t hnkm1, const uint64_t *hk, size_t hnk,
+                     uint64_t **out, size_t *nout) {
+    cudaStream_t st = g.stream;
+    uint64_t k = n >> i0;
+    int kodd = (int)(k & 1);
+    uint64_t nk = hnk ? hnk : 1, nkm1 = hnkm1 ? hnkm1 : 1;
+    uint64_t cap0 = std::max(nk, nkm1);
+    ALLOC(fk, uint64_t, cap0);
+    ALLOC(fkm1, uint64_t, cap0);
+    CK(cudaMemsetAsync(fk, 0, cap0 * 8, st));
+    CK(cudaMemsetAsync(fkm1, 0, cap0 * 8, st));
+    CK(cudaMemcpyAsync(fk, hk, hnk * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(fkm1, hkm1, hnkm1 * 8, cudaMemcpyHostToDevice, st));
+    uint64_t bk = bits_of(hk, hnk), bkm1 = bits_of(hkm1, hnkm1);
+    CK(cudaEventRecord(g.ev0, st));
+    for (int i = i0 - 1; i >= 1; i--) {
+        const int bit = (int)((n >> i) & 1);
+        if (bkm1 == 0) bkm1 = 1;
+        nk = (bk + 63) / 64, nkm1 = (bkm1 + 63) / 64;
+        const uint64_t n1 = 2 * nk + 1, n2 = 2 * nkm1 + 1;
+        ALLOC(s1, uint64_t, n1);
+        ALLOC(s2, uint64_t, n2);
+        Prod p1{fk, fk, nk, nk, bk, bk, s1, 0}, p2{fkm1, fkm1, nkm1, nkm1, bkm1, bkm1, s2, 0};
+        ffg_plan pl1, pl2;
+        int rc = plan_select(bk, bk, 1, &pl1);
+        if (!rc) rc = plan_select(bkm1, bkm1, 1, &pl2);
+        if (rc) return rc;
+        if (pl1.width == pl2.width && pl1.L == pl2.L && pl1.kernel == pl2.kernel && pl1.row_lg == pl2.row_lg) {
+            Prod pp[2] = {p1, p2};
+            rc = run_products(pp, 2, pl1, true, st);
+        } else {
+            rc = run_products(&p1, 1, pl1, true, st);
+            if (!rc) rc = run_products(&p2, 1, pl2, true, st);
+        }
+        if (rc) return rc;
+        // A = s1 + s2 = F(2k-1), B = 4 s1 - s2 + 2(-1)^k = F(2k+1), C = B - A = F(2k)
+        const uint64_t len = n1 + 1;
+        const int64_t pm2 = kodd ? -2 : 2;
+        ALLOC(lo, uint64_t, len);
+        ALLOC(hi, uint64_t, len);
+        if (bit) rc = lin(s1, n1, s2, n2, len, 2, lo, 3, -2, pm2, hi, 4, -1, pm2, st);
+        else rc = lin(s1, n1, s2, n2, len, 2, lo, 1, 1, 0, hi, 3, -2, pm2, st);
+        if (rc) return rc;
+        k = 2 * k + (uint64_t)bit;
+        kodd = bit;
+        fkm1 = lo;
+        fk = hi;
+        bk = fib_bits(k);
+        bkm1 = fib_bits(k - 1);
+    }
+    // last bit (src/fib.c:239-260)
+    nk = (bk + 63) / 64, nkm1 = (bkm1 + 63) / 64;
+    const uint64_t lenx = std::max(nk, nkm1) + 1;
+    uint64_t *res = nullptr;
+    uint64_t nres = 0;
+    int rc;
+    if (n & 1) {
+        ALLOC(x, uint64_t, lenx);
+        ALLOC(y, uint64_t, lenx);
+        rc = lin(fk, nk, fkm1, nkm1, lenx, 2, x, 2, 1, 0, y, 2, -1, 0, st);
+        if (rc) return rc;
+        uint64_t bx = fib_bits(k + 2);   // 2F(k) + F(k-1) = F(k+2)
+        uint64_t by = lucas_bits(k - 1); // 2F(k) - F(k-1) = F(k) + F(k-2) = L(k-1)
+        nres = 2 * lenx + 1;
+        ALLOC(r, uint64_t, nres);
+        res = r;
+        Prod p{x, y, lenx, lenx, bx, by, r, kodd ? -2 : 2};
+        rc = mul_one(p, false, st);
+    } else {
+        ALLOC(x, uint64_t, lenx);
+        rc = lin(fkm1, nkm1, fk, nk, lenx, 1, x, 2, 1, 0, nullptr, 0, 0, 0, st);
+        if (rc) return rc;
+        uint64_t bx = lucas_bits(k); // F(k) + 2F(k-1) = L(k)
+        nres = nk + lenx + 1;
+        ALLOC(r, uint64_t, nres);
+        res = r;
+        Prod p{fk, x, nk, lenx, bk, bx, r, 0};
+        rc = mul_one(p, false, st);
+    }
+    if (rc) return rc;
+    CK(cudaEventRecord(g.ev1, st));
+    uint64_t *h = (uint64_t *)malloc(nres * 8);
+    if (!h) return fail(FFG_E_NOMEM, "host: %zu bytes", (size_t)nres * 8);
+    CK(cudaMemcpyAsync(h, res, nres * 8, cudaMemcpyDeviceToHost, st));
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e) {
+        free(h);
+        return fail(FFG_E_CUDA, "fib chain: %s", cudaGetErrorString(e));
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, g.ev0, g.ev1);
+    g.chain_ms = ms;
+    while (nres > 1 && h[nres - 1] == 0) nres--;
+    *out = h;
+    *nout = nres;
+    return FFG_OK;
+}
+
+} // namespace ffg
+
+// =================================================================== C ABI
+
+using namespace ffg;
+
+extern "C" int ffg_init(size_t max_limbs) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    size_t L = 16;
+    while (L < 2 * max_limbs && L < ((size_t)1 << kMaxLg)) L <<= 1;
+    if (L > g.max_L) g.max_L = L;
+    return FFG_OK;
+}
+
+extern "C" size_t ffg_ntt_max_L(void) { return g.max_L; }
+extern "C" void ffg_set_ntt_max_L(size_t L) { g.max_L = L; }
+
+extern "C" int ffg_plan_select(uint64_t bits_a, uint64_t bits_b, int square, ffg_plan *plan) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (!plan) return fail(FFG_E_ARG, "plan is NULL");
+    int rc = plan_select(bits_a, bits_b, square, plan);
+    if (rc == FFG_E_RANGE && plan->split) return FFG_OK; // the plan says: split
+    return rc;
+}
+
+extern "C" int ffg_mul_device(uint64_t *out, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b,
+                              size_t nb, uint64_t bits_b, int square, void *stream) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!out || !a || (!square && !b) || na == 0 || (!square && nb == 0)) return fail(FFG_E_ARG, "bad arguments");
+    cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+    Prod p{a, square ? a : b, na, square ? na : nb, bits_a, square ? bits_a : bits_b, out, 0};
+    if (bits_a == 0 || (!square && bits_b == 0)) {
+        CK(cudaMemsetAsync(out, 0, (na + (square ? na : nb) + 1) * 8, st));
+        return FFG_OK;
+    }
+    arena_reset();
+    return mul_one(p, square != 0, st);
+}
+
+extern "C" int ffg_mul_host(uint64_t *out, size_t *nout, const uint64_t *a, size_t na, const uint64_t *b, size_t nb,
+                            int square) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (square) b = a, nb = na;
+    uint64_t ba = bits_of(a, na), bb = bits_of(b, nb);
+    if (ba == 0 || bb == 0) {
+        out[0] = 0;
+        *nout = 1;
+        return FFG_OK;
+    }
+    na = (ba + 63) / 64, nb = (bb + 63) / 64;
+    cudaStream_t st = g.stream;
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    ALLOC(da, uint64_t, na);
+    uint64_t *db = da;
+    if (!square) {
+        ALLOC(t, uint64_t, nb);
+        db = t;
+    }
+    const uint64_t nr = na + nb + 1;
+    ALLOC(dr, uint64_t, nr);
+    CK(cudaMemcpyAsync(da, a, na * 8, cudaMemcpyHostToDevice, st));
+    if (!square) CK(cudaMemcpyAsync(db, b, nb * 8, cudaMemcpyHostToDevice, st));
+    Prod p{da, db, na, nb, ba, bb, dr, 0};
+    rc = mul_one(p, square != 0, st);
+    if (rc) return rc;
+    std::vector<uint64_t> tmp(nr);
+    CK(cudaMemcpyAsync(tmp.data(), dr, nr * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    size_t n = na + nb;
+    while (n > 1 && tmp[n - 1] == 0) n--;
+    memcpy(out, tmp.data(), n * 8);
+    *nout = n;
+    return FFG_OK;
+}
+
+extern "C" int ffg_fib_chain(uint64_t n, int i0, const uint64_t *fkm1, size_t nkm1, const uint64_t *fk, size_t nk,
+                             uint64_t **out, size_t *nout) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (i0 < 1 || i0 > 63 || !fk || !out || !nout) return fail(FFG_E_ARG, "bad arguments");
+    CK(cudaStreamSynchronize(g.stream));
+    arena_reset();
+    return fib_chain(n, i0, fkm1, nkm1, fk, nk, out, nout);
+}
+
+extern "C" double ffg_last_chain_ms(void) { return g.chain_ms; }
+extern "C" const char *ffg_last_error(void) { return g.err.c_str(); }
+extern "C" void ffg_free(void *p) { free(p); }
+
+extern "C" void ffg_shutdown(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (!g.ready) return;
+    cudaStreamSynchronize(g.stream);
+    for (auto &b : g.blocks) cudaFree(b.ptr);
+    g.blocks.clear();
+    cudaFree(g.tables);
+    g.tables = nullptr;
+    cudaEventDestroy(g.ev0);
+    cudaEventDestroy(g.ev1);
+    cudaStreamDestroy(g.stream);
+    g.ready = false;
+}

@@ -1,0 +1,187 @@
+// NTT convolution kernels for sm_100a: three primes, lengths L = 2^k and
+// 3 2^k, operands read straight from 64-bit limbs.
+//
+// Short lengths (L <= 2^FFG_LINE_LG words) run one CTA per (product, prime)
+// with the whole transform in shared memory: load digits, forward, pointwise,
+// inverse, scale (k_conv_small).  This is the reference's in-cache
+// convolution (src/ntt_conv.c:205-226, src/ntt_kernels.c:274-295) as one
+// kernel, and the batched path of the decimal conversion and uneven streams.
+//
+// Long lengths use the four-step split L = R x C (C = 2^c contiguous "rows"
+// of the residue array, R = 2^r or 3 2^r "columns"):
+//   k_col_fwd  : digits of a column tile -> length-R forward transforms down
+//                the columns -> twiddle ω_L^(n2 k1) -> residues, row-major
+//   k_row_conv : per row: forward length-C transform of both operands,
+//                pointwise product, inverse, twiddle ω_L^-(n2 k1)
+//   k_col_inv  : inverse length-R transforms down the columns, scale by
+//                2^32 / L, natural coefficient order for the CRT
+// The reference's top radix-16 passes over column chunks and in-cache
+// sub-blocks (src/ntt_conv.c:158-226) play the same roles on the CPU; here
+// each pass is one HBM round trip of the residues.
+#include "ffg_device.cuh"
+#include "ffg_internal.h"
+
+namespace ffg {
+
+// ------------------------------------------------------------ short lengths
+
+__global__ void __launch_bounds__(256) k_conv_small(Primes3 P3, const ConvJob *__restrict__ jobs) {
+    extern __shared__ uint32_t smem[];
+    const ConvJob J = jobs[blockIdx.x];
+    const PrimeDev P = P3.pr[blockIdx.y];
+    const uint32_t L = J.L_words, p = P.p;
+    const uint32_t stride = line_stride(L);
+    uint32_t *fa = smem, *fb = smem + stride;
+    const bool sq = J.square != 0;
+
+    for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) {
+        fa[pad_idx(i)] = i < J.ca ? reduce_digit(digit_at(J.a, J.na, i, J.width), P) : 0;
+        if (!sq) fb[pad_idx(i)] = i < J.cb ? reduce_digit(digit_at(J.b, J.nb, i, J.width), P) : 0;
+    }
+    __syncthreads();
+    LineSet ls{sq ? 1u : 2u, J.n, J.r3, stride};
+    lines_forward(smem, ls, P);
+    for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) {
+        uint32_t x = fa[pad_idx(i)];
+        fa[pad_idx(i)] = mont(x, sq ? x : fb[pad_idx(i)], p, P.pinv);
+    }
+    __syncthreads();
+    ls.lines = 1;
+    lines_inverse(smem, ls, P);
+    const uint32_t scl = J.scl[blockIdx.y], scls = J.scls[blockIdx.y];
+    uint32_t *y = J.y + (size_t)blockIdx.y * J.y_stride;
+    for (uint32_t i = threadIdx.x; i < J.conv; i += blockDim.x) y[i] = shoup(fa[pad_idx(i)], scl, scls, p);
+}
+
+// ------------------------------------------------------------- four-step
+
+// Column tile: columns [c0, c0 + wc) of all R rows, wc lines of length R.
+__global__ void __launch_bounds__(256) k_col_fwd(Primes3 P3, FourStep G, const FSJob *__restrict__ jobs) {
+    extern __shared__ uint32_t smem[];
+    const uint32_t z = blockIdx.z, op = G.square ? 0 : (z & 1), jb = G.square ? z : (z >> 1);
+    const FSJob J = jobs[jb];
+    const PrimeDev P = P3.pr[blockIdx.y];
+    const uint32_t R = G.R, C = 1u << G.c, wc = G.wc, stride = G.col_stride;
+    const uint32_t c0 = blockIdx.x * wc;
+    const uint64_t *src = op ? J.b : J.a;
+    const uint64_t ns = op ? J.nb : J.na, cs = op ? J.cb : J.ca;
+
+    for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
+        uint32_t n1 = idx / wc, c = idx % wc;
+        uint64_t i = (uint64_t)n1 * C + c0 + c;
+        smem[c * stride + pad_idx(n1)] = i < cs ? reduce_digit(digit_at(src, ns, i, J.width), P) : 0;
+    }
+    __syncthreads();
+    LineSet ls{wc, G.rn, G.r3, stride};
+    lines_forward(smem, ls, P);
+    uint32_t *y = (op ? J.yb : J.ya) + (size_t)blockIdx.y * G.L;
+    for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
+        uint32_t pos = idx / wc, c = idx % wc;
+        uint32_t k1 = freq_of(pos, G.rn, G.r3), n2 = c0 + c;
+        uint64_t E = (uint64_t)n2 * k1 * G.mstep;
+        uint32_t v = smem[c * stride + pad_idx(pos)];
+        y[(size_t)pos * C + n2] = mont(v, tw_mont(P, E), P.p, P.pinv);
+    }
+}
+
+// One row (position pos of the column transform) per CTA.
+__global__ void __launch_bounds__(256) k_row_conv(Primes3 P3, FourStep G, const FSJob *__restrict__ jobs) {
+    extern __shared__ uint32_t smem[];
+    const FSJob J = jobs[blockIdx.z];
+    const PrimeDev P = P3.pr[blockIdx.y];
+    const uint32_t C = 1u << G.c, pos = blockIdx.x, p = P.p;
+    const uint32_t stride = line_stride(C);
+    const bool sq = G.square != 0;
+    uint32_t *ya = J.ya + (size_t)blockIdx.y * G.L + (size_t)pos * C;
+    const uint32_t *yb = sq ? ya : J.yb + (size_t)blockIdx.y * G.L + (size_t)pos * C;
+    uint32_t *fa = smem, *fb = smem + stride;
+
+    for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
+        fa[pad_idx(i)] = ya[i];
+        if (!sq) fb[pad_idx(i)] = yb[i];
+    }
+    __syncthreads();
+    LineSet ls{sq ? 1u : 2u, G.c, 0, stride};
+    lines_forward(smem, ls, P);
+    for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
+        uint32_t x = fa[pad_idx(i)];
+        fa[pad_idx(i)] = mont(x, sq ? x : fb[pad_idx(i)], p, P.pinv);
+    }
+    __syncthreads();
+    ls.lines = 1;
+    lines_inverse(smem, ls, P);
+    const uint32_t k1 = freq_of(pos, G.rn, G.r3);
+    for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
+        uint64_t E = (uint64_t)i * k1 * G.mstep;
+        E = E ? FFG_M - E : 0; // ω^-e = ω^(M - E)
+        ya[i] = mont(fa[pad_idx(i)], tw_mont(P, E), p, P.pinv);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_col_inv(Primes3 P3, FourStep G, const FSJob *__restrict__ jobs) {
+    extern __shared__ uint32_t smem[];
+    const FSJob J = jobs[blockIdx.z];
+    const PrimeDev P = P3.pr[blockIdx.y];
+    const uint32_t R = G.R, C = 1u << G.c, wc = G.wc, stride = G.col_stride;
+    const uint32_t c0 = blockIdx.x * wc;
+    uint32_t *y = J.ya + (size_t)blockIdx.y * G.L;
+
+    for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
+        uint32_t pos = idx / wc, c = idx % wc;
+        smem[c * stride + pad_idx(pos)] = y[(size_t)pos * C + c0 + c];
+    }
+    __syncthreads();
+    LineSet ls{wc, G.rn, G.r3, stride};
+    lines_inverse(smem, ls, P);
+    const uint32_t scl = G.scl[blockIdx.y], scls = G.scls[blockIdx.y];
+    for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
+        uint32_t n1 = idx / wc, c = idx % wc;
+        y[(size_t)n1 * C + c0 + c] = shoup(smem[c * stride + pad_idx(n1)], scl, scls, P.p);
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+
+static size_t small_smem_bytes(uint32_t L, bool square) {
+    return (size_t)line_stride(L) * (square ? 1 : 2) * sizeof(uint32_t);
+}
+
+cudaError_t launch_conv_small(const Primes3 &P3, const ConvJob *d_jobs, uint32_t njobs, uint32_t maxL,
+                              bool any_distinct, cudaStream_t st) {
+    size_t sm = small_smem_bytes(maxL, !any_distinct);
+    static size_t configured = 0;
+    if (sm > configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_conv_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        configured = sm;
+    }
+    k_conv_small<<<dim3(njobs, 3, 1), 256, sm, st>>>(P3, d_jobs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *d_jobs, uint32_t njobs,
+                             cudaStream_t st) {
+    static size_t cfg_col = 0, cfg_row = 0;
+    size_t sm_col = (size_t)G.col_stride * G.wc * sizeof(uint32_t);
+    size_t sm_row = (size_t)line_stride(1u << G.c) * (G.square ? 1 : 2) * sizeof(uint32_t);
+    cudaError_t e;
+    if (sm_col > cfg_col) {
+        if ((e = cudaFuncSetAttribute(k_col_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_col))) return e;
+        if ((e = cudaFuncSetAttribute(k_col_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_col))) return e;
+        cfg_col = sm_col;
+    }
+    if (sm_row > cfg_row) {
+        if ((e = cudaFuncSetAttribute(k_row_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_row))) return e;
+        cfg_row = sm_row;
+    }
+    const uint32_t C = 1u << G.c, tiles = C / G.wc;
+    const uint32_t nops = G.square ? 1 : 2;
+    k_col_fwd<<<dim3(tiles, 3, njobs * nops), 256, sm_col, st>>>(P3, G, d_jobs);
+    if ((e = cudaGetLastError())) return e;
+    k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, d_jobs);
+    if ((e = cudaGetLastError())) return e;
+    k_col_inv<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, d_jobs);
+    return cudaGetLastError();
+}
+
+} // namespace ffg

@@ -1,0 +1,89 @@
+/*
+ * ffg.h -- the thin C ABI of the B200 layer (libfastfib_b200.so).
+ *
+ * Plain C types only: sizes, limb pointers (little-endian 64-bit limbs, as
+ * the reference's Big, src/common.h:29-33) and an opaque stream handle
+ * (a cudaStream_t, or NULL for the library's own stream).  Every function
+ * returns 0 on success and a nonzero FFG_E* code on failure; ffg_last_error()
+ * then describes the failure.  Calls are serialized by one lock, so the host
+ * surface may call in from several threads (the reference calls big_sqr from
+ * two pool tasks at once, src/fib.c:184-198).
+ *
+ * The entry points replace the reference's internal NTT interface; each
+ * comment names the reference function whose job it takes over.
+ */
+#ifndef FFG_H
+#define FFG_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    FFG_OK = 0,
+    FFG_E_CUDA = 1,     /* a CUDA runtime call failed */
+    FFG_E_NOMEM = 2,    /* device or host allocation failed */
+    FFG_E_ARG = 3,      /* invalid argument (size, width, length) */
+    FFG_E_NODEV = 4,    /* no CUDA device */
+    FFG_E_RANGE = 5     /* a size past what this entry point supports */
+};
+
+/* The plan of one NTT product: what big_mul_ntt (src/mul_ntt.c:97-118) or the
+   split (src/mul_split.c:149-177) would choose, plus the GPU geometry. */
+typedef struct {
+    uint32_t width;   /* coefficient bits b, 32..35 (split: 8..35) */
+    uint32_t lg;      /* transform length L = 2^lg, or 3 * 2^lg when r3 */
+    uint32_t r3;
+    uint32_t split;   /* 1: piecewise split multiply */
+    uint64_t L;       /* transform length (split: the piece length Lp) */
+    uint64_t conv;    /* product coefficients ca + cb - 1 */
+    uint64_t ca, cb;
+    uint64_t ka, kb;  /* split: pieces per operand */
+    uint64_t Lbig;    /* split: (ka + kb) * Lp / 2 */
+    uint32_t kernel;  /* 0: one-CTA transform, 1: four-step */
+    uint32_t row_lg;  /* four-step: log2 of the row length */
+} ffg_plan;
+
+/* ntt_init (src/ntt_tables.c:72): sizes the transform cap for products of up
+   to max_limbs limbs (2^k >= 2 max_limbs, at most 2^25) and builds the device
+   tables on first use.  The cap only grows. */
+int ffg_init(size_t max_limbs);
+/* g_ntt_max_L (src/mul_basic.c:26): read and override the transform cap (the
+   reference's tests set it to force paths, tests/nttfuzz.c:33-39). */
+size_t ffg_ntt_max_L(void);
+void ffg_set_ntt_max_L(size_t L);
+/* big_mul_ntt's choice of width, length and split (src/mul_ntt.c:97-118). */
+int ffg_plan_select(uint64_t bits_a, uint64_t bits_b, int square, ffg_plan *plan);
+
+/* big_mul_ntt (src/mul_ntt.c:97) on host limbs: out receives na + nb limbs
+   at most (normalized length in *nout).  square != 0 multiplies a by itself
+   (the reference signals it by a == b). */
+int ffg_mul_host(uint64_t *out, size_t *nout, const uint64_t *a, size_t na, const uint64_t *b, size_t nb,
+                 int square);
+/* big_mul_ntt on device limbs.  bits_a / bits_b: bit lengths (upper bounds
+   are allowed; leading zero limbs are fine).  out: na + nb + 1 limbs of
+   device memory, fully written.  stream: a cudaStream_t or NULL. */
+int ffg_mul_device(uint64_t *out, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b, size_t nb,
+                   uint64_t bits_b, int square, void *stream);
+
+/* fibonacci (src/fib.c:211) from bit i0 down: continues fast doubling from
+   the pair (F(k-1), F(k)), k = n >> i0, on the device and returns F(n) as a
+   malloc'ed limb array (free with ffg_free).  i0 >= 1. */
+int ffg_fib_chain(uint64_t n, int i0, const uint64_t *fkm1, size_t nkm1, const uint64_t *fk, size_t nk,
+                  uint64_t **out, size_t *nout);
+
+/* Device timing of the last ffg_fib_chain call, in milliseconds (CUDA events
+   around the chain on its stream; excludes the host prefix and copies). */
+double ffg_last_chain_ms(void);
+
+const char *ffg_last_error(void);
+void ffg_free(void *p);
+/* Releases device memory, streams and tables. */
+void ffg_shutdown(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

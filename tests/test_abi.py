@@ -1,0 +1,63 @@
+"""CPU tests of the boundary: the library builds, loads without a GPU, and
+exports every function declared in include/*.h; the plan logic is host-only
+and checked against the oracle's restatement of big_mul_ntt's choice."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INC = os.path.join(ROOT, "include")
+
+
+def declared_functions():
+    names = set()
+    for fn in os.listdir(INC):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(INC, fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(", text, flags=re.M):
+            name = m.group(1)
+            if name not in ("if", "while", "for", "return", "sizeof"):
+                names.add(name)
+    return names
+
+
+def test_header_has_the_reference_surface():
+    names = declared_functions()
+    for n in ("big_mul", "big_sqr", "big_mul_ntt", "fibonacci", "big_to_string", "ntt_init", "big_free",
+              "ffg_init", "ffg_mul_host", "ffg_mul_device", "ffg_fib_chain", "ffg_plan_select", "ffg_last_error"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol(ff):
+    lib = ff.lib()
+    missing = [n for n in sorted(declared_functions()) if not hasattr(lib, n)]
+    assert not missing, missing
+    ctypes.c_size_t.in_dll(lib, "g_ntt_max_L")  # the reference's global, exported too
+
+
+def test_plan_select_without_gpu(ff, oracle):
+    """Plans need no device: they mirror big_mul_ntt's width / length choice."""
+    oracle.ntt_init(1 << 22)
+    ff.lib().ffg_set_ntt_max_L(oracle.ntt_max_L())
+    for bits_a, bits_b in ((6400, 6400), (64 * 1356, 64 * 1356), (64 * 5424, 64 * 5424), (64 * 10000, 64 * 333),
+                           (64 * 542377, 64 * 542377), (64 * 271189, 64 * 271189), (100, 64 * 2000)):
+        for sq in ((True, False) if bits_a == bits_b else (False,)):
+            p = ff.plan(bits_a, bits_b, sq)
+            o = oracle.plan(bits_a, bits_b, sq)
+            assert (p["width"], p["L"], p["lg"], p["r3"], p["conv"]) == (o.width, o.L, o.lg, o.r3, o.conv)
+
+
+def test_gpu_calls_fail_loudly_without_gpu(ff):
+    import numpy as np
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(ff.FfgError):
+        ff.mul(np.ones(300, dtype=np.uint64))
