@@ -69,6 +69,12 @@ def lib() -> ctypes.CDLL:
     L.ffg_fib_chain.argtypes = [ctypes.c_uint64, ctypes.c_int, _u64p, ctypes.c_size_t, _u64p,
                                 ctypes.c_size_t, ctypes.POINTER(_u64p), _szp]
     L.ffg_last_chain_ms.restype = ctypes.c_double
+    L.ffg_profile.argtypes = [ctypes.c_uint32]
+    L.ffg_last_chain_io.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.ffg_set_device.argtypes = [ctypes.c_int]
+    L.ffg_profile_read.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]
+    L.ffg_launch_count.restype = ctypes.c_uint64
     L.ffg_last_error.restype = ctypes.c_char_p
     L.ffg_free.argtypes = [ctypes.c_void_p]
     for name in ("big_mul", "big_mul_ntt", "big_mul_toom3"):
@@ -216,3 +222,41 @@ def fib_chain(n: int, i0: int, fkm1, fk) -> np.ndarray:
 
 def last_chain_ms() -> float:
     return lib().ffg_last_chain_ms()
+
+
+KERNEL_FAMILIES = ("conv_small", "col_fwd", "row_conv", "col_inv", "crt", "carry", "lin")
+
+
+def profile(families=None) -> None:
+    """Resets the per-family totals; brackets the named kernel families (all
+    when families is True, none when falsy) with CUDA events from now on."""
+    if families is True:
+        mask = (1 << len(KERNEL_FAMILIES)) - 1
+    elif not families:
+        mask = 0
+    else:
+        mask = sum(1 << KERNEL_FAMILIES.index(f) for f in families)
+    lib().ffg_profile(mask)
+
+
+def last_chain_io() -> tuple:
+    h, d = ctypes.c_uint64(), ctypes.c_uint64()
+    lib().ffg_last_chain_io(ctypes.byref(h), ctypes.byref(d))
+    return h.value, d.value
+
+
+def set_device(device: int) -> None:
+    _check(lib().ffg_set_device(device))
+
+
+def profile_read() -> dict:
+    out = {}
+    for k, name in enumerate(KERNEL_FAMILIES):
+        n, ms, by = ctypes.c_uint64(), ctypes.c_double(), ctypes.c_double()
+        _check(lib().ffg_profile_read(k, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by)))
+        out[name] = {"launches": n.value, "ms": ms.value, "bytes": by.value}
+    return out
+
+
+def launch_count() -> int:
+    return lib().ffg_launch_count()

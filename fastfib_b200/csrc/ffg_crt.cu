@@ -126,10 +126,12 @@ cudaError_t launch_scan_apply(uint64_t *out, uint64_t nlimbs, uint32_t chunk_lim
                               uint32_t cta_chunks, const StepFn *pref, const StepFn *cta_fn, __int128 *cta_in,
                               int64_t c0, cudaStream_t st) {
     const uint32_t ncta = (nchunks + cta_chunks - 1) / cta_chunks;
+    prof_begin(PK_CARRY, st);
     k_scan_ctas<<<1, 32, 0, st>>>(cta_fn, ncta, c0, cta_in);
     cudaError_t e = cudaGetLastError();
     if (e) return e;
     k_apply_carry<<<(nchunks + 255) / 256, 256, 0, st>>>(out, nlimbs, chunk_limbs, nchunks, cta_chunks, pref, cta_in);
+    prof_end(PK_CARRY, st, (double)nchunks * (sizeof(StepFn) + 32));
     return cudaGetLastError();
 }
 
@@ -143,7 +145,9 @@ cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st) {
         configured = true;
     }
     const uint32_t ncta = (J.nchunks + FFG_CRT_THREADS - 1) / FFG_CRT_THREADS;
+    prof_begin(PK_CRT, st);
     k_crt_chunks<<<ncta, FFG_CRT_THREADS, sm, st>>>(garner_const(), J);
+    prof_end(PK_CRT, st, 12.0 * (double)J.conv + 8.0 * (double)J.nlimbs);
     cudaError_t e = cudaGetLastError();
     if (e) return e;
     return launch_scan_apply(J.out, J.nlimbs, J.width, J.nchunks, FFG_CRT_THREADS, J.pref, J.cta_fn, J.cta_in,
@@ -193,7 +197,9 @@ __global__ void __launch_bounds__(FFG_LIN_THREADS) k_lin_chunks(LinJob J) {
 
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st) {
     const uint32_t ncta = (J.nchunks + FFG_LIN_THREADS - 1) / FFG_LIN_THREADS;
+    prof_begin(PK_LIN, st);
     k_lin_chunks<<<ncta, FFG_LIN_THREADS, 0, st>>>(J);
+    prof_end(PK_LIN, st, 8.0 * (double)(J.n1 + J.n2) + 8.0 * (double)J.len * J.nout);
     cudaError_t e = cudaGetLastError();
     if (e) return e;
     for (uint32_t k = 0; k < J.nout; k++) {

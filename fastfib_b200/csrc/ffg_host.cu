@@ -67,10 +67,74 @@ struct Ctx {
     std::string err;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double chain_ms = 0;
+    uint64_t chain_h2d = 0, chain_d2h = 0;
+    int device = -1;
 };
 
 static Ctx g;
 static std::recursive_mutex g_mu;
+
+// ------------------------------------------------------------ profiling
+
+// Launch counter (always on) and, when enabled, CUDA-event brackets around
+// every launch of each kernel family, on the stream the kernel runs on.
+struct ProfPair {
+    int kind;
+    cudaEvent_t a, b;
+    double bytes;
+};
+static uint64_t g_launches = 0;
+static bool g_prof_on = false;
+static uint32_t g_prof_mask = 0;
+static std::vector<ProfPair> g_prof_open;
+static std::vector<cudaEvent_t> g_ev_pool;
+static double g_prof_ms[PK_COUNT], g_prof_bytes[PK_COUNT];
+static uint64_t g_prof_n[PK_COUNT];
+
+static cudaEvent_t ev_get() {
+    if (!g_ev_pool.empty()) {
+        cudaEvent_t e = g_ev_pool.back();
+        g_ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void prof_begin(int kind, cudaStream_t st) {
+    g_launches++;
+    if (!g_prof_on || !((g_prof_mask >> kind) & 1)) return;
+    ProfPair pp{kind, ev_get(), nullptr, 0};
+    cudaEventRecord(pp.a, st);
+    g_prof_open.push_back(pp);
+}
+
+void prof_end(int kind, cudaStream_t st, double bytes) {
+    if (!g_prof_on || !((g_prof_mask >> kind) & 1)) return;
+    if (g_prof_open.empty() || g_prof_open.back().kind != kind || g_prof_open.back().b) return;
+    ProfPair &pp = g_prof_open.back();
+    pp.b = ev_get();
+    pp.bytes = bytes;
+    cudaEventRecord(pp.b, st);
+}
+
+// Folds finished brackets into the totals (synchronizes on their events).
+static void prof_collect() {
+    for (auto &pp : g_prof_open) {
+        if (pp.b) {
+            float ms = 0;
+            cudaEventSynchronize(pp.b);
+            cudaEventElapsedTime(&ms, pp.a, pp.b);
+            g_prof_ms[pp.kind] += ms;
+            g_prof_bytes[pp.kind] += pp.bytes;
+            g_prof_n[pp.kind]++;
+            g_ev_pool.push_back(pp.b);
+        }
+        g_ev_pool.push_back(pp.a);
+    }
+    g_prof_open.clear();
+}
 
 static int fail(int code, const char *fmt, ...) {
     char buf[512];
@@ -156,9 +220,13 @@ static int build_tables() {
 }
 
 static int ensure_ready() {
-    if (g.ready) return FFG_OK;
+    if (g.ready) {
+        if (g.device >= 0) CK(cudaSetDevice(g.device));
+        return FFG_OK;
+    }
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(FFG_E_NODEV, "no CUDA device");
+    if (g.device >= 0) CK(cudaSetDevice(g.device));
     CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&g.ev0));
     CK(cudaEventCreate(&g.ev1));
@@ -316,7 +384,8 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
             memcpy(J.scls, scls, sizeof scls);
             ALLOC(dj, ConvJob, 1);
             CK(cudaMemcpyAsync(dj, &J, sizeof J, cudaMemcpyHostToDevice, st));
-            e = launch_conv_small(g.P3, dj, 1, (uint32_t)L, !square, st);
+            e = launch_conv_small(g.P3, dj, 1, (uint32_t)L, !square, st,
+                                  8.0 * (double)(J.na + (square ? 0 : J.nb)) + 12.0 * (double)J.conv);
             if (e) return fail(FFG_E_CUDA, "conv_small: %s", cudaGetErrorString(e));
         }
     } else {
@@ -348,7 +417,9 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
         }
         ALLOC(dj, FSJob, count);
         CK(cudaMemcpyAsync(dj, jobs.data(), count * sizeof(FSJob), cudaMemcpyHostToDevice, st));
-        e = launch_four_step(g.P3, G, dj, (uint32_t)count, st);
+        double limb_bytes = 0;
+        for (int i = 0; i < count; i++) limb_bytes += 8.0 * (double)(jobs[i].na + (square ? 0 : jobs[i].nb));
+        e = launch_four_step(g.P3, G, dj, (uint32_t)count, st, limb_bytes);
         if (e) return fail(FFG_E_CUDA, "four_step: %s", cudaGetErrorString(e));
     }
     for (int i = 0; i < count; i++) {
@@ -520,6 +591,8 @@ static int fib_chain(uint64_t n, int i0, const uint64_t *hkm1, size_t hnkm1, con
     float ms = 0;
     cudaEventElapsedTime(&ms, g.ev0, g.ev1);
     g.chain_ms = ms;
+    g.chain_h2d = 8 * (uint64_t)(hnk + hnkm1);
+    g.chain_d2h = 8 * nres;
     while (nres > 1 && h[nres - 1] == 0) nres--;
     *out = h;
     *nout = nres;
@@ -620,6 +693,40 @@ extern "C" int ffg_fib_chain(uint64_t n, int i0, const uint64_t *fkm1, size_t nk
 }
 
 extern "C" double ffg_last_chain_ms(void) { return g.chain_ms; }
+
+extern "C" void ffg_last_chain_io(uint64_t *h2d_bytes, uint64_t *d2h_bytes) {
+    *h2d_bytes = g.chain_h2d;
+    *d2h_bytes = g.chain_d2h;
+}
+
+extern "C" int ffg_set_device(int device) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (g.ready && device != g.device) return fail(FFG_E_ARG, "device already chosen (%d)", g.device);
+    g.device = device;
+    if (!g.ready) return FFG_OK;
+    CK(cudaSetDevice(device));
+    return FFG_OK;
+}
+
+extern "C" void ffg_profile(uint32_t mask) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    prof_collect();
+    g_prof_on = mask != 0;
+    g_prof_mask = mask;
+    for (int k = 0; k < PK_COUNT; k++) g_prof_ms[k] = g_prof_bytes[k] = 0, g_prof_n[k] = 0;
+}
+
+extern "C" int ffg_profile_read(int kind, uint64_t *launches, double *ms, double *bytes) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (kind < 0 || kind >= PK_COUNT) return fail(FFG_E_ARG, "profile kind %d", kind);
+    prof_collect();
+    *launches = g_prof_n[kind];
+    *ms = g_prof_ms[kind];
+    *bytes = g_prof_bytes[kind];
+    return FFG_OK;
+}
+
+extern "C" uint64_t ffg_launch_count(void) { return g_launches; }
 extern "C" const char *ffg_last_error(void) { return g.err.c_str(); }
 extern "C" void ffg_free(void *p) { free(p); }
 

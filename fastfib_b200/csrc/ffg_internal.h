@@ -94,11 +94,19 @@ constexpr uint32_t FFG_LIN_K = 8;         // limbs per thread in the linear kern
 constexpr uint32_t FFG_LIN_THREADS = 256;
 
 cudaError_t launch_conv_small(const Primes3 &P3, const ConvJob *d_jobs, uint32_t njobs, uint32_t maxL,
-                              bool any_distinct, cudaStream_t st);
+                              bool any_distinct, cudaStream_t st, double bytes);
 cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *d_jobs, uint32_t njobs,
-                             cudaStream_t st);
+                             cudaStream_t st, double limb_bytes);
 cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st);
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st);
+
+// Kernel families the profiler tracks (ffg_profile_read in include/ffg.h).
+enum ProfKind { PK_CONV_SMALL = 0, PK_COL_FWD, PK_ROW_CONV, PK_COL_INV, PK_CRT, PK_CARRY, PK_LIN, PK_COUNT };
+
+// Brackets one kernel launch on stream st with CUDA events when profiling is
+// on, and counts launches always.  bytes: the launch's algorithmic bytes.
+void prof_begin(int kind, cudaStream_t st);
+void prof_end(int kind, cudaStream_t st, double bytes);
 
 struct GarnerConst {
     uint32_t p[3];

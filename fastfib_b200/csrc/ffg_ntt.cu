@@ -147,7 +147,7 @@ static size_t small_smem_bytes(uint32_t L, bool square) {
 }
 
 cudaError_t launch_conv_small(const Primes3 &P3, const ConvJob *d_jobs, uint32_t njobs, uint32_t maxL,
-                              bool any_distinct, cudaStream_t st) {
+                              bool any_distinct, cudaStream_t st, double bytes) {
     size_t sm = small_smem_bytes(maxL, !any_distinct);
     static size_t configured = 0;
     if (sm > configured) {
@@ -155,12 +155,14 @@ cudaError_t launch_conv_small(const Primes3 &P3, const ConvJob *d_jobs, uint32_t
         if (e != cudaSuccess) return e;
         configured = sm;
     }
+    prof_begin(PK_CONV_SMALL, st);
     k_conv_small<<<dim3(njobs, 3, 1), 256, sm, st>>>(P3, d_jobs);
+    prof_end(PK_CONV_SMALL, st, bytes);
     return cudaGetLastError();
 }
 
 cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *d_jobs, uint32_t njobs,
-                             cudaStream_t st) {
+                             cudaStream_t st, double limb_bytes) {
     static size_t cfg_col = 0, cfg_row = 0;
     size_t sm_col = (size_t)G.col_stride * G.wc * sizeof(uint32_t);
     size_t sm_row = (size_t)line_stride(1u << G.c) * (G.square ? 1 : 2) * sizeof(uint32_t);
@@ -176,11 +178,20 @@ cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *
     }
     const uint32_t C = 1u << G.c, tiles = C / G.wc;
     const uint32_t nops = G.square ? 1 : 2;
+    // algorithmic bytes: one 4-byte read and write of every residue per pass
+    // (twiddles excluded); the first pass reads limbs instead of residues
+    const double res = 3.0 * 4.0 * (double)G.L * njobs;
+    prof_begin(PK_COL_FWD, st);
     k_col_fwd<<<dim3(tiles, 3, njobs * nops), 256, sm_col, st>>>(P3, G, d_jobs);
+    prof_end(PK_COL_FWD, st, res * nops + limb_bytes);
     if ((e = cudaGetLastError())) return e;
+    prof_begin(PK_ROW_CONV, st);
     k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, d_jobs);
+    prof_end(PK_ROW_CONV, st, res * (nops + 1));
     if ((e = cudaGetLastError())) return e;
+    prof_begin(PK_COL_INV, st);
     k_col_inv<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, d_jobs);
+    prof_end(PK_COL_INV, st, res * 2);
     return cudaGetLastError();
 }
 

@@ -77,6 +77,23 @@ int ffg_fib_chain(uint64_t n, int i0, const uint64_t *fkm1, size_t nkm1, const u
 /* Device timing of the last ffg_fib_chain call, in milliseconds (CUDA events
    around the chain on its stream; excludes the host prefix and copies). */
 double ffg_last_chain_ms(void);
+/* Bytes the last ffg_fib_chain copied host -> device and device -> host. */
+void ffg_last_chain_io(uint64_t *h2d_bytes, uint64_t *d2h_bytes);
+
+/* Selects the CUDA device for every later call (one process per GPU); call
+   before the first other entry point. */
+int ffg_set_device(int device);
+
+/* Kernel-family profiling for the roofline: with profiling on, every launch
+   of a family is bracketed by CUDA events on its own stream; read returns the
+   launches, summed device milliseconds and summed algorithmic bytes since
+   ffg_profile() was last called.  Families: 0 one-CTA convolution, 1 forward
+   column pass, 2 row pass (forward, pointwise, inverse), 3 inverse column
+   pass, 4 CRT, 5 carry settle, 6 linear pass. */
+void ffg_profile(uint32_t family_mask); /* bit k on: bracket family k; 0: off */
+int ffg_profile_read(int kind, uint64_t *launches, double *ms, double *bytes);
+/* Kernel launches made by the library since it was loaded. */
+uint64_t ffg_launch_count(void);
 
 const char *ffg_last_error(void);
 void ffg_free(void *p);

@@ -300,7 +300,8 @@ static void split_plan(uint64_t bits_a, uint64_t bits_b, int square, FoPlan *pl)
     unsigned bw = 35;
     while (bw > 8 && !width_ok(bits_a, bits_b, bw)) bw--;
     size_t cap = g_max_L < ((size_t)1 << MAX_LG) ? g_max_L : ((size_t)1 << MAX_LG);
-    int lgmax = cap ? __builtin_ctzll(cap) : 0;
+    if (cap < 16) cap = 16; /* no tables yet: the smallest ntt_init builds 16 */
+    int lgmax = __builtin_ctzll(cap);
     int lgp = lgmax;
     double best = 0;
     for (int lg = lgmax; lg >= lgmax - 4 && lg >= 10; lg--) {

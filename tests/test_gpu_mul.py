@@ -86,6 +86,7 @@ def test_all_ones_square(ff, nlimbs):
 
 def test_lengths_both_families(ff, oracle):
     """Sizes whose plan lands on 2^k and on 3 * 2^k, one-CTA and four-step."""
+    oracle.ntt_init(1 << 22)
     rng = np.random.default_rng(7)
     seen = set()
     for n in [60, 100, 130, 190, 260, 400, 700, 1000, 1500, 2100, 3000, 4200, 6000, 9000, 13000, 20000,
