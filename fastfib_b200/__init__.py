@@ -72,6 +72,8 @@ def lib() -> ctypes.CDLL:
     L.ffg_profile.argtypes = [ctypes.c_uint32]
     L.ffg_last_chain_io.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.ffg_set_device.argtypes = [ctypes.c_int]
+    L.ffg_set_max_lg.argtypes = [ctypes.c_int]
+    L.ff_set_max_lg.argtypes = [ctypes.c_int]
     L.ffg_profile_read.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_double)]
     L.ffg_launch_count.restype = ctypes.c_uint64
@@ -140,6 +142,12 @@ def set_g_ntt_max_L(L: int) -> None:
 
 def ntt_init(max_limbs: int) -> None:
     lib().ntt_init(max_limbs)
+
+
+def set_max_lg(lg: int) -> None:
+    """The reference's NTT_MAX_LG at run time (25 by default): lower values send
+    long products to the split multiply (its -DNTT_MAX_LG=23 / 12 / 10 builds)."""
+    _check(lib().ff_set_max_lg(lg))
 
 
 def big_mul(a, b) -> np.ndarray:

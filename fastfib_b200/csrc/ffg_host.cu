@@ -20,7 +20,7 @@ typedef unsigned __int128 u128h;
 
 static const uint32_t kP[3] = {2113929217u, 2013265921u, 1811939329u}; // src/ntt_arith.c:48-52
 static const uint32_t kG[3] = {5u, 31u, 13u};
-static const int kMaxLg = 25;                                           // NTT_MAX_LG, src/common.h:46-48
+static int kMaxLg = 25; // NTT_MAX_LG (src/common.h:46-48); ffg_set_max_lg lowers it like -DNTT_MAX_LG
 static const uint32_t kSmallMaxL = 4096;  // one-CTA transform up to this length for a single product
 static const int kR3TabLg = 13;           // radix-3 tables cover R = 3 2^n, n < 13
 
@@ -299,15 +299,48 @@ static uint64_t ntt_length(uint64_t conv, uint32_t *lg_out, uint32_t *r3_out) {
 }
 
 static void gpu_geometry(ffg_plan *pl) {
-    if (pl->L <= kSmallMaxL) {
+    if (pl->L <= kSmallMaxL && !pl->split) {
         pl->kernel = 0;
         pl->row_lg = 0;
         return;
     }
     int c = (int)pl->lg - 7;
     c = c < 8 ? 8 : (c > 13 ? 13 : c);
+    if (c > (int)pl->lg) c = (int)pl->lg;
     pl->kernel = 1;
     pl->row_lg = (uint32_t)c;
+}
+
+// The split's width and piece length (src/mul_split.c:150-177): the widest
+// width the CRT bound allows, then the piece length 2^lg over the last five
+// lengths by the reference's cost model (tr lg + 5 pairs) 2^lg.
+static void split_plan(uint64_t bits_a, uint64_t bits_b, int square, ffg_plan *pl) {
+    unsigned bw = 35;
+    while (bw > 8 && !width_ok(bits_a, bits_b, bw)) bw--;
+    size_t cap = g.max_L < ((size_t)1 << kMaxLg) ? g.max_L : ((size_t)1 << kMaxLg);
+    if (cap < 16) cap = 16;
+    int lgmax = __builtin_ctzll(cap), lgp = lgmax;
+    double best = 0;
+    for (int lg = lgmax; lg >= lgmax - 4 && lg >= 10; lg--) {
+        uint64_t h = (uint64_t)1 << (lg - 1);
+        uint64_t ka = ((bits_a + bw - 1) / bw + h - 1) / h, kb = ((bits_b + bw - 1) / bw + h - 1) / h;
+        double ca = (double)ka, cb = (double)kb;
+        double tr = square ? 3 * ca - 1 : 2 * (ca + cb) - 1, pairs = square ? ca * (ca + 1) / 2 : ca * cb;
+        double cost = (tr * lg + 5 * pairs) * (double)((uint64_t)1 << lg);
+        if (lg == lgmax || cost < best) best = cost, lgp = lg;
+    }
+    const uint64_t Lp = (uint64_t)1 << lgp, H = Lp / 2;
+    memset(pl, 0, sizeof *pl);
+    pl->split = 1;
+    pl->width = bw;
+    pl->lg = (uint32_t)lgp;
+    pl->L = Lp;
+    pl->ca = (bits_a + bw - 1) / bw;
+    pl->cb = (bits_b + bw - 1) / bw;
+    pl->ka = (pl->ca + H - 1) / H;
+    pl->kb = square ? pl->ka : (pl->cb + H - 1) / H;
+    pl->conv = pl->ca + pl->cb - 1;
+    pl->Lbig = (pl->ka + pl->kb) * H;
 }
 
 static int plan_select(uint64_t bits_a, uint64_t bits_b, int square, ffg_plan *pl) {
@@ -324,12 +357,7 @@ static int plan_select(uint64_t bits_a, uint64_t bits_b, int square, ffg_plan *p
             pl->ca = ca, pl->cb = cb, pl->conv = ca + cb - 1;
         }
     }
-    (void)square;
-    if (L == 0 || L > g.max_L) {
-        pl->split = 1;
-        return fail(FFG_E_RANGE, "product of %llu x %llu bits needs the split multiply (L=%llu > cap %zu)",
-                    (unsigned long long)bits_a, (unsigned long long)bits_b, (unsigned long long)L, g.max_L);
-    }
+    if (L == 0 || L > g.max_L) split_plan(bits_a, bits_b, square, pl);
     gpu_geometry(pl);
     return FFG_OK;
 }
@@ -352,6 +380,26 @@ struct Prod {
     uint64_t *out;   // na + nb + 1 limbs
     int64_t add;     // small constant added to the product
 };
+
+static FourStep four_step_geometry(const ffg_plan &pl, bool square) {
+    FourStep G{};
+    G.L = pl.L;
+    G.c = pl.row_lg;
+    G.rn = pl.lg - G.c;
+    G.r3 = pl.r3;
+    G.R = (pl.r3 ? 3u : 1u) << G.rn;
+    uint32_t wc = 32768u / G.R;
+    wc = wc < 8 ? 8 : (wc > 64 ? 64 : wc);
+    while (wc & (wc - 1)) wc &= wc - 1;
+    if (wc > (1u << G.c)) wc = 1u << G.c;
+    G.wc = wc;
+    G.col_stride = line_stride(G.R);
+    G.square = square;
+    G.mode = ROW_CONV;
+    G.mstep = FFG_M / pl.L;
+    scale_consts(pl.L, G.scl, G.scls);
+    return G;
+}
 
 // Products that share one plan (same width, length, squareness), run as one
 // batch of transforms, then one CRT each.
@@ -389,22 +437,7 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
             if (e) return fail(FFG_E_CUDA, "conv_small: %s", cudaGetErrorString(e));
         }
     } else {
-        FourStep G{};
-        G.L = L;
-        G.c = pl.row_lg;
-        G.rn = pl.lg - G.c;
-        G.r3 = pl.r3;
-        G.R = (pl.r3 ? 3u : 1u) << G.rn;
-        uint32_t wc = 32768u / G.R;
-        wc = wc < 8 ? 8 : (wc > 64 ? 64 : wc);
-        while (wc & (wc - 1)) wc &= wc - 1;
-        if (wc > (1u << G.c)) wc = 1u << G.c;
-        G.wc = wc;
-        G.col_stride = line_stride(G.R);
-        G.square = square;
-        G.mstep = FFG_M / L;
-        memcpy(G.scl, scl, sizeof scl);
-        memcpy(G.scls, scls, sizeof scls);
+        FourStep G = four_step_geometry(pl, square);
         std::vector<FSJob> jobs(count);
         for (int i = 0; i < count; i++) {
             FSJob &J = jobs[i];
@@ -444,11 +477,84 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
     return FFG_OK;
 }
 
+// The piecewise split multiply (src/mul_split.c:98-187) on the device: every
+// piece of H = Lp/2 coefficients transformed once; per output piece m the
+// pointwise sum over i + j = m, one inverse, added into the product's
+// residues at m H; then one CRT over all of them.
+static int run_split(const Prod &pr, bool square, const ffg_plan &pl, cudaStream_t st) {
+    const uint64_t Lp = pl.L, H = Lp / 2, ka = pl.ka, kb = pl.kb, Lyst = pl.Lbig + Lp;
+    const uint32_t w = pl.width;
+    FourStep G = four_step_geometry(pl, true);
+    ALLOC(A, uint32_t, ka * 3 * Lp);
+    uint32_t *B = A;
+    if (!square) {
+        ALLOC(Bt, uint32_t, kb * 3 * Lp);
+        B = Bt;
+    }
+    ALLOC(Cb, uint32_t, 3 * Lp);
+    ALLOC(Y, uint32_t, 3 * Lyst);
+    CK(cudaMemsetAsync(Y, 0, 3 * Lyst * sizeof(uint32_t), st));
+    const uint64_t np = ka + (square ? 0 : kb), nm = ka + kb - 1;
+    std::vector<FSJob> jobs(np + nm);
+    double limb_bytes = 0;
+    for (uint64_t i = 0; i < np; i++) {
+        const bool isb = i >= ka;
+        const uint64_t k = isb ? i - ka : i, tot = isb ? pl.cb : pl.ca;
+        FSJob &J = jobs[i];
+        J.a = isb ? pr.b : pr.a;
+        J.na = isb ? pr.nb : pr.na;
+        J.off_a = k * H;
+        J.ca = tot > k * H ? std::min(H, tot - k * H) : 0;
+        J.ya = (isb ? B : A) + k * 3 * Lp;
+        J.width = w;
+        limb_bytes += (double)J.ca * w / 8.0;
+    }
+    for (uint64_t m = 0; m < nm; m++) {
+        FSJob &J = jobs[np + m];
+        J.pa = A;
+        J.pb = B;
+        J.piece_stride = 3 * Lp;
+        J.m = (uint32_t)m, J.ka = (uint32_t)ka, J.kb = (uint32_t)kb, J.psq = square;
+        J.ya = Cb;
+        J.yacc = Y;
+        J.acc_off = m * H;
+        J.acc_stride = Lyst;
+        J.width = w;
+    }
+    ALLOC(dj, FSJob, jobs.size());
+    CK(cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(FSJob), cudaMemcpyHostToDevice, st));
+    cudaError_t e = launch_split_forward(g.P3, G, dj, (uint32_t)np, st, limb_bytes);
+    if (e) return fail(FFG_E_CUDA, "split forward: %s", cudaGetErrorString(e));
+    for (uint64_t m = 0; m < nm; m++) {
+        const uint64_t i0 = m + 1 > kb ? m + 1 - kb : 0, i1 = std::min(m, ka - 1);
+        e = launch_split_piece(g.P3, G, dj + np + m, (uint32_t)(i1 - i0 + 1), st);
+        if (e) return fail(FFG_E_CUDA, "split piece %llu: %s", (unsigned long long)m, cudaGetErrorString(e));
+    }
+    CrtJob C{};
+    C.y = Y;
+    C.y_stride = Lyst;
+    C.conv = pl.conv;
+    C.out = pr.out;
+    C.nlimbs = pr.na + (square ? pr.na : pr.nb) + 1;
+    C.width = w;
+    C.nchunks = (uint32_t)((C.nlimbs + w - 1) / w);
+    C.add = pr.add;
+    const uint32_t ncta = (C.nchunks + FFG_CRT_THREADS - 1) / FFG_CRT_THREADS;
+    C.pref = (StepFn *)arena_alloc((size_t)C.nchunks * sizeof(StepFn));
+    C.cta_fn = (StepFn *)arena_alloc((size_t)ncta * sizeof(StepFn));
+    C.cta_in = (__int128 *)arena_alloc((size_t)ncta * sizeof(__int128));
+    if (!C.pref || !C.cta_fn || !C.cta_in) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
+    e = launch_crt(g.P3, C, st);
+    if (e) return fail(FFG_E_CUDA, "crt: %s", cudaGetErrorString(e));
+    return FFG_OK;
+}
+
 // One product on device limbs (plan from the bit lengths).
 static int mul_one(const Prod &p, bool square, cudaStream_t st) {
     ffg_plan pl;
     int rc = plan_select(p.bits_a, square ? p.bits_a : p.bits_b, square, &pl);
     if (rc) return rc;
+    if (pl.split) return run_split(p, square, pl, st);
     return run_products(&p, 1, pl, square, st);
 }
 
@@ -526,7 +632,11 @@ static int fib_chain(uint64_t n, int i0, const uint64_t *hkm1, size_t hnkm1, con
         int rc = plan_select(bk, bk, 1, &pl1);
         if (!rc) rc = plan_select(bkm1, bkm1, 1, &pl2);
         if (rc) return rc;
-        if (pl1.width == pl2.width && pl1.L == pl2.L && pl1.kernel == pl2.kernel && pl1.row_lg == pl2.row_lg) {
+        if (pl1.split || pl2.split) {
+            rc = mul_one(p1, true, st);
+            if (!rc) rc = mul_one(p2, true, st);
+        } else if (pl1.width == pl2.width && pl1.L == pl2.L && pl1.kernel == pl2.kernel &&
+                   pl1.row_lg == pl2.row_lg) {
             Prod pp[2] = {p1, p2};
             rc = run_products(pp, 2, pl1, true, st);
         } else {
@@ -616,13 +726,20 @@ extern "C" int ffg_init(size_t max_limbs) {
 }
 
 extern "C" size_t ffg_ntt_max_L(void) { return g.max_L; }
+
+extern "C" int ffg_set_max_lg(int lg) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (lg < 4 || lg > 25) return fail(FFG_E_ARG, "max lg %d outside 4..25", lg);
+    kMaxLg = lg;
+    if (g.max_L > ((size_t)1 << lg)) g.max_L = (size_t)1 << lg;
+    return FFG_OK;
+}
 extern "C" void ffg_set_ntt_max_L(size_t L) { g.max_L = L; }
 
 extern "C" int ffg_plan_select(uint64_t bits_a, uint64_t bits_b, int square, ffg_plan *plan) {
     std::lock_guard<std::recursive_mutex> lk(g_mu);
     if (!plan) return fail(FFG_E_ARG, "plan is NULL");
     int rc = plan_select(bits_a, bits_b, square, plan);
-    if (rc == FFG_E_RANGE && plan->split) return FFG_OK; // the plan says: split
     return rc;
 }
 

@@ -30,6 +30,13 @@ struct ConvJob {
     uint32_t scl[3], scls[3]; // 2^32 / L mod p (Shoup pairs)
 };
 
+// What the row pass does (FourStep::mode).
+enum RowMode : uint32_t {
+    ROW_CONV = 0,    // forward both operands, pointwise product, inverse
+    ROW_FWD = 1,     // forward only, in place (the split's transformed pieces)
+    ROW_ACC_INV = 2, // sum of piece products for one output piece, inverse
+};
+
 // Geometry of a four-step launch (shared by its jobs).
 struct FourStep {
     uint64_t L;             // transform length = R * 2^c
@@ -38,17 +45,28 @@ struct FourStep {
     uint32_t wc;            // columns per CTA in the column passes
     uint32_t col_stride;    // shared words per column line
     uint32_t square;
+    uint32_t mode;          // RowMode of k_row_conv
     uint64_t mstep;         // M / L
     uint32_t scl[3], scls[3];
 };
 
 // One product of a four-step launch.  ya / yb: 3 * L words each (prime-major);
-// ya ends holding the scaled convolution in natural order.
+// ya ends holding the scaled convolution in natural order.  The split's
+// pieces read digits [off, off + ca) of their operand.  With yacc set, the
+// inverse column pass adds its result into yacc[acc_off ..] (per prime
+// acc_stride words) instead of writing ya: the split's overlap-add.
 struct FSJob {
     const uint64_t *a, *b;
     uint64_t na, nb, ca, cb;
     uint32_t *ya, *yb;
     uint32_t width, pad;
+    uint64_t off_a, off_b;
+    // ROW_ACC_INV: output piece m = sum_{i+j=m} A_i B_j over transformed pieces
+    const uint32_t *pa, *pb;  // piece i at pa + i * piece_stride
+    uint64_t piece_stride;
+    uint32_t m, ka, kb, psq;  // psq: pb == pa, pairs i <= j counted twice when i < j
+    uint32_t *yacc;
+    uint64_t acc_off, acc_stride;
 };
 
 // A chunk's (or a run of chunks') carry map c_in -> c_out: a step function
@@ -97,6 +115,9 @@ cudaError_t launch_conv_small(const Primes3 &P3, const ConvJob *d_jobs, uint32_t
                               bool any_distinct, cudaStream_t st, double bytes);
 cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *d_jobs, uint32_t njobs,
                              cudaStream_t st, double limb_bytes);
+cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJob *d_jobs, uint32_t njobs,
+                                 cudaStream_t st, double limb_bytes);
+cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob *d_job, uint32_t pairs, cudaStream_t st);
 cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st);
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st);
 

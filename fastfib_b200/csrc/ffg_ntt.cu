@@ -64,12 +64,12 @@ __global__ void __launch_bounds__(256) k_col_fwd(Primes3 P3, FourStep G, const F
     const uint32_t R = G.R, C = 1u << G.c, wc = G.wc, stride = G.col_stride;
     const uint32_t c0 = blockIdx.x * wc;
     const uint64_t *src = op ? J.b : J.a;
-    const uint64_t ns = op ? J.nb : J.na, cs = op ? J.cb : J.ca;
+    const uint64_t ns = op ? J.nb : J.na, cs = op ? J.cb : J.ca, off = op ? J.off_b : J.off_a;
 
     for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
         uint32_t n1 = idx / wc, c = idx % wc;
         uint64_t i = (uint64_t)n1 * C + c0 + c;
-        smem[c * stride + pad_idx(n1)] = i < cs ? reduce_digit(digit_at(src, ns, i, J.width), P) : 0;
+        smem[c * stride + pad_idx(n1)] = i < cs ? reduce_digit(digit_at(src, ns, off + i, J.width), P) : 0;
     }
     __syncthreads();
     LineSet ls{wc, G.rn, G.r3, stride};
@@ -84,7 +84,11 @@ __global__ void __launch_bounds__(256) k_col_fwd(Primes3 P3, FourStep G, const F
     }
 }
 
-// One row (position pos of the column transform) per CTA.
+// One row (position pos of the column transform) per CTA.  ROW_CONV: forward
+// transform of the row of both operands, pointwise product, inverse.
+// ROW_FWD: forward transform only (the split's pieces).  ROW_ACC_INV: the
+// split's output piece m, sum over i + j = m of A_i B_j on this row
+// (src/mul_split.c:62-78), then the inverse.
 __global__ void __launch_bounds__(256) k_row_conv(Primes3 P3, FourStep G, const FSJob *__restrict__ jobs) {
     extern __shared__ uint32_t smem[];
     const FSJob J = jobs[blockIdx.z];
@@ -96,19 +100,46 @@ __global__ void __launch_bounds__(256) k_row_conv(Primes3 P3, FourStep G, const 
     const uint32_t *yb = sq ? ya : J.yb + (size_t)blockIdx.y * G.L + (size_t)pos * C;
     uint32_t *fa = smem, *fb = smem + stride;
 
-    for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
-        fa[pad_idx(i)] = ya[i];
-        if (!sq) fb[pad_idx(i)] = yb[i];
+    if (G.mode == ROW_ACC_INV) {
+        const uint64_t rowoff = (size_t)blockIdx.y * G.L + (size_t)pos * C;
+        const uint32_t m = J.m;
+        const uint32_t i0 = m + 1 > J.kb ? m + 1 - J.kb : 0;
+        uint32_t i1 = m < J.ka - 1 ? m : J.ka - 1;
+        if (J.psq && i1 > m / 2) i1 = m / 2;
+        for (uint32_t t = threadIdx.x; t < C; t += blockDim.x) {
+            uint32_t acc = 0;
+            for (uint32_t i = i0; i <= i1; i++) {
+                const uint32_t j = m - i;
+                uint32_t v = mont(J.pa[i * J.piece_stride + rowoff + t], J.pb[j * J.piece_stride + rowoff + t], p,
+                                  P.pinv);
+                acc = add_mod(acc, v, p);
+                if (J.psq && i < j) acc = add_mod(acc, v, p);
+            }
+            fa[pad_idx(t)] = acc;
+        }
+        __syncthreads();
+    } else {
+        for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
+            fa[pad_idx(i)] = ya[i];
+            if (!sq) fb[pad_idx(i)] = yb[i];
+        }
+        __syncthreads();
+        LineSet lf{sq ? 1u : 2u, G.c, 0, stride};
+        lines_forward(smem, lf, P);
+        if (G.mode == ROW_FWD) {
+            for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
+                ya[i] = fa[pad_idx(i)];
+                if (!sq) ((uint32_t *)yb)[i] = fb[pad_idx(i)];
+            }
+            return;
+        }
+        for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
+            uint32_t x = fa[pad_idx(i)];
+            fa[pad_idx(i)] = mont(x, sq ? x : fb[pad_idx(i)], p, P.pinv);
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    LineSet ls{sq ? 1u : 2u, G.c, 0, stride};
-    lines_forward(smem, ls, P);
-    for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
-        uint32_t x = fa[pad_idx(i)];
-        fa[pad_idx(i)] = mont(x, sq ? x : fb[pad_idx(i)], p, P.pinv);
-    }
-    __syncthreads();
-    ls.lines = 1;
+    LineSet ls{1u, G.c, 0, stride};
     lines_inverse(smem, ls, P);
     const uint32_t k1 = freq_of(pos, G.rn, G.r3);
     for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
@@ -134,6 +165,15 @@ __global__ void __launch_bounds__(256) k_col_inv(Primes3 P3, FourStep G, const F
     LineSet ls{wc, G.rn, G.r3, stride};
     lines_inverse(smem, ls, P);
     const uint32_t scl = G.scl[blockIdx.y], scls = G.scls[blockIdx.y];
+    if (J.yacc) { // overlap-add of a split output piece
+        uint32_t *acc = J.yacc + (size_t)blockIdx.y * J.acc_stride + J.acc_off;
+        for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
+            uint32_t n1 = idx / wc, c = idx % wc;
+            const size_t at = (size_t)n1 * C + c0 + c;
+            acc[at] = add_mod(acc[at], shoup(smem[c * stride + pad_idx(n1)], scl, scls, P.p), P.p);
+        }
+        return;
+    }
     for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
         uint32_t n1 = idx / wc, c = idx % wc;
         y[(size_t)n1 * C + c0 + c] = shoup(smem[c * stride + pad_idx(n1)], scl, scls, P.p);
@@ -192,6 +232,64 @@ cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *
     prof_begin(PK_COL_INV, st);
     k_col_inv<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, d_jobs);
     prof_end(PK_COL_INV, st, res * 2);
+    return cudaGetLastError();
+}
+
+// The split multiply's passes, each over a list of jobs sharing geometry G.
+static cudaError_t cfg_four_step(const FourStep &G, size_t *sm_col, size_t *sm_row) {
+    static size_t cfg_col = 0, cfg_row = 0;
+    *sm_col = (size_t)G.col_stride * G.wc * sizeof(uint32_t);
+    *sm_row = (size_t)line_stride(1u << G.c) * (G.square ? 1 : 2) * sizeof(uint32_t);
+    cudaError_t e;
+    if (*sm_col > cfg_col) {
+        if ((e = cudaFuncSetAttribute(k_col_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*sm_col))) return e;
+        if ((e = cudaFuncSetAttribute(k_col_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*sm_col))) return e;
+        cfg_col = *sm_col;
+    }
+    if (*sm_row > cfg_row) {
+        if ((e = cudaFuncSetAttribute(k_row_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*sm_row))) return e;
+        cfg_row = *sm_row;
+    }
+    return cudaSuccess;
+}
+
+// Forward transforms of njobs pieces (one operand each, G.square = 1).
+cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJob *d_jobs, uint32_t njobs,
+                                 cudaStream_t st, double limb_bytes) {
+    size_t sm_col, sm_row;
+    G.square = 1;
+    G.mode = ROW_FWD;
+    cudaError_t e = cfg_four_step(G, &sm_col, &sm_row);
+    if (e) return e;
+    const uint32_t tiles = (1u << G.c) / G.wc;
+    const double res = 3.0 * 4.0 * (double)G.L * njobs;
+    prof_begin(PK_COL_FWD, st);
+    k_col_fwd<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, d_jobs);
+    prof_end(PK_COL_FWD, st, res + limb_bytes);
+    if ((e = cudaGetLastError())) return e;
+    prof_begin(PK_ROW_CONV, st);
+    k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, d_jobs);
+    prof_end(PK_ROW_CONV, st, res * 2);
+    return cudaGetLastError();
+}
+
+// One output piece: pairwise sum + inverse row pass, then the inverse column
+// pass adding into the whole product's residues.  pairs: products summed.
+cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob *d_job, uint32_t pairs, cudaStream_t st) {
+    size_t sm_col, sm_row;
+    G.square = 1;
+    G.mode = ROW_ACC_INV;
+    cudaError_t e = cfg_four_step(G, &sm_col, &sm_row);
+    if (e) return e;
+    const uint32_t tiles = (1u << G.c) / G.wc;
+    const double res = 3.0 * 4.0 * (double)G.L;
+    prof_begin(PK_ROW_CONV, st);
+    k_row_conv<<<dim3(G.R, 3, 1), 256, sm_row, st>>>(P3, G, d_job);
+    prof_end(PK_ROW_CONV, st, res * (2.0 * pairs + 1.0));
+    if ((e = cudaGetLastError())) return e;
+    prof_begin(PK_COL_INV, st);
+    k_col_inv<<<dim3(tiles, 3, 1), 256, sm_col, st>>>(P3, G, d_job);
+    prof_end(PK_COL_INV, st, res * 3.0);
     return cudaGetLastError();
 }
 

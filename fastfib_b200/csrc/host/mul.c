@@ -33,8 +33,19 @@ void ntt_init(size_t max_limbs) {
     ffg_set_ntt_max_L(g_ntt_max_L);
 }
 
+int ff_max_lg = NTT_MAX_LG; /* lowered by ffg_set_max_lg through ff_set_max_lg */
+
 static int ntt_fits(const Big *a, const Big *b) {
-    return 2 * (a->n + b->n) - 1 <= g_ntt_max_L || g_ntt_max_L >= ((size_t)1 << NTT_MAX_LG);
+    return 2 * (a->n + b->n) - 1 <= g_ntt_max_L || g_ntt_max_L >= ((size_t)1 << ff_max_lg);
+}
+
+/* The run-time NTT_MAX_LG of this surface and of the GPU layer together. */
+int ff_set_max_lg(int lg) {
+    int rc = ffg_set_max_lg(lg);
+    if (rc) return rc;
+    ff_max_lg = lg;
+    if (g_ntt_max_L > ((size_t)1 << lg)) g_ntt_max_L = (size_t)1 << lg;
+    return 0;
 }
 
 Big big_mul_ntt(const Big *a, const Big *b) {

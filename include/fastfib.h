@@ -63,6 +63,8 @@ Big big_mul_schoolbook(const Big *a, const Big *b);
 Big big_sqr_schoolbook(const Big *a);
 
 void ntt_init(size_t max_limbs);
+/* The run-time counterpart of the reference's -DNTT_MAX_LG (default 25). */
+int ff_set_max_lg(int lg);
 Big big_mul(const Big *a, const Big *b);
 Big big_sqr(const Big *a);
 Big big_mul_ntt(const Big *a, const Big *b);

@@ -54,6 +54,10 @@ int ffg_init(size_t max_limbs);
    reference's tests set it to force paths, tests/nttfuzz.c:33-39). */
 size_t ffg_ntt_max_L(void);
 void ffg_set_ntt_max_L(size_t L);
+/* NTT_MAX_LG (src/common.h:46-48) at run time: the longest transform 2^lg
+   (4..25, default 25); lower values send long products to the split
+   multiply, as the reference's -DNTT_MAX_LG builds do (tests/test.ps1:29). */
+int ffg_set_max_lg(int lg);
 /* big_mul_ntt's choice of width, length and split (src/mul_ntt.c:97-118). */
 int ffg_plan_select(uint64_t bits_a, uint64_t bits_b, int square, ffg_plan *plan);
 

@@ -133,10 +133,14 @@ class Oracle(_Lib):
         super().__init__(path)
         self.lib.fo_ntt_plan.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(FoPlan)]
         self.lib.fo_ntt_plan.restype = ctypes.c_int
+        self.lib.fo_set_max_lg.argtypes = [ctypes.c_int]
         self.lib.fo_fingerprint.argtypes = [_u64p, ctypes.c_size_t, _u64p]
         self.lib.fo_mul_ntt_forced.restype = ctypes.c_void_p
         self.lib.fo_mul_ntt_forced.argtypes = [_u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, ctypes.c_int,
                                                ctypes.c_uint32, ctypes.c_uint64, _szp]
+
+    def set_max_lg(self, lg: int) -> None:
+        self.lib.fo_set_max_lg(lg)
 
     def plan(self, bits_a: int, bits_b: int, square: bool = False) -> FoPlan:
         p = FoPlan()

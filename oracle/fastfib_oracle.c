@@ -244,7 +244,7 @@ static Num mul_school(const Num *a, const Num *b) {
 
 /* ------------------------------------------------------- NTT definitions */
 
-#define MAX_LG 25 /* NTT_MAX_LG (src/common.h:46-48) */
+static int MAX_LG = 25; /* NTT_MAX_LG (src/common.h:46-48); fo_set_max_lg mirrors -DNTT_MAX_LG */
 static const uint32_t P[3] = {2113929217u, 2013265921u, 1811939329u}; /* src/ntt_arith.c:48-52 */
 static const uint32_t G[3] = {5, 31, 13};
 
@@ -268,6 +268,10 @@ void fo_ntt_init(size_t max_limbs) {
     if (L > g_max_L) g_max_L = L;
 }
 size_t fo_ntt_max_L(void) { return g_max_L; }
+void fo_set_max_lg(int lg) {
+    MAX_LG = lg;
+    if (g_max_L > ((size_t)1 << lg)) g_max_L = (size_t)1 << lg;
+}
 void fo_set_ntt_max_L(size_t L) { g_max_L = L; }
 
 /* ntt_width_ok (src/mul_ntt.c:55-59) */

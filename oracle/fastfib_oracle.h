@@ -38,6 +38,7 @@ typedef struct {
 void fo_ntt_init(size_t max_limbs);
 size_t fo_ntt_max_L(void);
 void fo_set_ntt_max_L(size_t L);
+void fo_set_max_lg(int lg); /* the reference's -DNTT_MAX_LG, at run time */
 int fo_ntt_plan(uint64_t bits_a, uint64_t bits_b, int square, FoPlan *plan);
 
 uint64_t *fo_mul(const uint64_t *a, size_t na, const uint64_t *b, size_t nb, int square, size_t *nout);
