@@ -227,6 +227,7 @@ static int ensure_ready() {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(FFG_E_NODEV, "no CUDA device");
     if (g.device >= 0) CK(cudaSetDevice(g.device));
+    else CK(cudaGetDevice(&g.device)); // the device this context is created on
     CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&g.ev0));
     CK(cudaEventCreate(&g.ev1));
@@ -860,3 +861,4 @@ extern "C" void ffg_shutdown(void) {
     cudaStreamDestroy(g.stream);
     g.ready = false;
 }
+

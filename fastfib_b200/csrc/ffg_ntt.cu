@@ -182,6 +182,23 @@ __global__ void __launch_bounds__(256) k_col_inv(Primes3 P3, FourStep G, const F
 
 // ---------------------------------------------------------------- launchers
 
+// Opts every kernel of this file into the device's largest dynamic shared
+// memory once; each launch then asks for what it needs.
+static cudaError_t smem_optin() {
+    static int done = 0;
+    if (done) return cudaSuccess;
+    int dev = 0, maxsm = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev))) return e;
+    if ((e = cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+    const void *ks[] = {(const void *)k_conv_small, (const void *)k_col_fwd, (const void *)k_row_conv,
+                        (const void *)k_col_inv};
+    for (const void *k : ks)
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    done = 1;
+    return cudaSuccess;
+}
+
 static size_t small_smem_bytes(uint32_t L, bool square) {
     return (size_t)line_stride(L) * (square ? 1 : 2) * sizeof(uint32_t);
 }
@@ -189,12 +206,8 @@ static size_t small_smem_bytes(uint32_t L, bool square) {
 cudaError_t launch_conv_small(const Primes3 &P3, const ConvJob *d_jobs, uint32_t njobs, uint32_t maxL,
                               bool any_distinct, cudaStream_t st, double bytes) {
     size_t sm = small_smem_bytes(maxL, !any_distinct);
-    static size_t configured = 0;
-    if (sm > configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_conv_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        configured = sm;
-    }
+    cudaError_t e = smem_optin();
+    if (e != cudaSuccess) return e;
     prof_begin(PK_CONV_SMALL, st);
     k_conv_small<<<dim3(njobs, 3, 1), 256, sm, st>>>(P3, d_jobs);
     prof_end(PK_CONV_SMALL, st, bytes);
@@ -203,19 +216,10 @@ cudaError_t launch_conv_small(const Primes3 &P3, const ConvJob *d_jobs, uint32_t
 
 cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *d_jobs, uint32_t njobs,
                              cudaStream_t st, double limb_bytes) {
-    static size_t cfg_col = 0, cfg_row = 0;
     size_t sm_col = (size_t)G.col_stride * G.wc * sizeof(uint32_t);
     size_t sm_row = (size_t)line_stride(1u << G.c) * (G.square ? 1 : 2) * sizeof(uint32_t);
-    cudaError_t e;
-    if (sm_col > cfg_col) {
-        if ((e = cudaFuncSetAttribute(k_col_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_col))) return e;
-        if ((e = cudaFuncSetAttribute(k_col_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_col))) return e;
-        cfg_col = sm_col;
-    }
-    if (sm_row > cfg_row) {
-        if ((e = cudaFuncSetAttribute(k_row_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_row))) return e;
-        cfg_row = sm_row;
-    }
+    cudaError_t e = smem_optin();
+    if (e) return e;
     const uint32_t C = 1u << G.c, tiles = C / G.wc;
     const uint32_t nops = G.square ? 1 : 2;
     // algorithmic bytes: one 4-byte read and write of every residue per pass
@@ -237,20 +241,9 @@ cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *
 
 // The split multiply's passes, each over a list of jobs sharing geometry G.
 static cudaError_t cfg_four_step(const FourStep &G, size_t *sm_col, size_t *sm_row) {
-    static size_t cfg_col = 0, cfg_row = 0;
     *sm_col = (size_t)G.col_stride * G.wc * sizeof(uint32_t);
     *sm_row = (size_t)line_stride(1u << G.c) * (G.square ? 1 : 2) * sizeof(uint32_t);
-    cudaError_t e;
-    if (*sm_col > cfg_col) {
-        if ((e = cudaFuncSetAttribute(k_col_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*sm_col))) return e;
-        if ((e = cudaFuncSetAttribute(k_col_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*sm_col))) return e;
-        cfg_col = *sm_col;
-    }
-    if (*sm_row > cfg_row) {
-        if ((e = cudaFuncSetAttribute(k_row_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*sm_row))) return e;
-        cfg_row = *sm_row;
-    }
-    return cudaSuccess;
+    return smem_optin();
 }
 
 // Forward transforms of njobs pieces (one operand each, G.square = 1).
