@@ -862,3 +862,120 @@ extern "C" void ffg_shutdown(void) {
     g.ready = false;
 }
 
+// ======================================================= allocation-free multiply
+//
+// ffg_mul_device_noalloc: the NTT product of ffg_mul_device for callers that
+// must not allocate device memory once they are running -- code executing
+// while a CUDA graph is being captured on its stream, a framework that owns
+// all device memory through its own allocator, or a latency-critical path
+// that cannot afford a cudaMalloc (and the device-wide synchronization it may
+// imply).  Its scratch (the residue arrays, the job record and the CRT's carry
+// maps) lives in the fixed array below, which every GPU that loads this
+// library holds until the process exits; products whose scratch would not fit
+// are rejected with FFG_E_RANGE.  The device tables are built once by
+// ffg_init, which the caller runs during its own set-up; this entry point
+// itself calls no cudaMalloc, cudaFree or other allocating routine.
+
+static constexpr size_t kNoAllocBytes = (size_t)8 << 20; // 8 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+static void *g_noalloc_addr[64]; // the array's device address, per device
+
+// Host code may not use g_noalloc_scratch's name as an address (it is a host
+// stand-in); the device address comes from cudaGetSymbolAddress, looked up
+// once per device with that device current.
+static int noalloc_address(int dev, void **addr) {
+    if (dev < 0 || dev >= 64) return fail(FFG_E_ARG, "device %d out of range", dev);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return fail(FFG_E_CUDA, "cudaGetSymbolAddress(allocation-free scratch): %s", cudaGetErrorString(e));
+        g_noalloc_addr[dev] = p;
+    }
+    *addr = g_noalloc_addr[dev];
+    return FFG_OK;
+}
+
+static size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+extern "C" int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t na, uint64_t bits_a,
+                                      const uint64_t *b, size_t nb, uint64_t bits_b, int square, void *stream) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (!g.ready) return fail(FFG_E_ARG, "ffg_mul_device_noalloc: call ffg_init during set-up first");
+    if (!out || !a || (!square && !b) || na == 0 || (!square && nb == 0)) return fail(FFG_E_ARG, "bad arguments");
+    if (g.device >= 0) CK(cudaSetDevice(g.device));
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    void *base = nullptr;
+    int rc = noalloc_address(dev, &base);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+    if (square) b = a, nb = na, bits_b = bits_a;
+    const uint64_t nlimbs = na + nb + 1;
+    if (bits_a == 0 || bits_b == 0) {
+        CK(cudaMemsetAsync(out, 0, nlimbs * 8, st));
+        return FFG_OK;
+    }
+    ffg_plan pl;
+    rc = plan_select(bits_a, bits_b, square, &pl);
+    if (rc) return rc;
+    if (pl.split) return fail(FFG_E_RANGE, "ffg_mul_device_noalloc: the product needs the split multiply");
+
+    // scratch layout: job record | residues of a | residues of b | CRT carry maps
+    const uint64_t L = pl.L;
+    const uint32_t w = pl.width;
+    const uint32_t nchunks = (uint32_t)((nlimbs + w - 1) / w);
+    const uint32_t ncta = (nchunks + FFG_CRT_THREADS - 1) / FFG_CRT_THREADS;
+    const size_t o_job = 0;
+    const size_t o_ya = o_job + up256(std::max(sizeof(ConvJob), sizeof(FSJob)));
+    const size_t o_yb = o_ya + up256(3 * L * sizeof(uint32_t));
+    const size_t o_pref = o_yb + (square ? 0 : up256(3 * L * sizeof(uint32_t)));
+    const size_t o_fn = o_pref + up256((size_t)nchunks * sizeof(StepFn));
+    const size_t o_in = o_fn + up256((size_t)ncta * sizeof(StepFn));
+    const size_t need = o_in + up256((size_t)ncta * sizeof(__int128));
+    if (need > kNoAllocBytes)
+        return fail(FFG_E_RANGE,
+                    "ffg_mul_device_noalloc: %llu x %llu bits needs %zu bytes of scratch, the limit is %zu bytes",
+                    (unsigned long long)bits_a, (unsigned long long)bits_b, need, kNoAllocBytes);
+    char *s = (char *)base;
+    uint32_t *ya = (uint32_t *)(s + o_ya), *yb = square ? nullptr : (uint32_t *)(s + o_yb);
+    const uint64_t ca = (bits_a + w - 1) / w, cb = (bits_b + w - 1) / w;
+    cudaError_t e;
+    if (pl.kernel == 0) {
+        ConvJob J{};
+        J.a = a, J.b = b, J.na = na, J.nb = nb, J.ca = ca, J.cb = cb;
+        J.y = ya;
+        J.y_stride = L;
+        J.L_words = (uint32_t)L;
+        J.n = pl.lg, J.r3 = pl.r3, J.width = w, J.square = square != 0;
+        J.conv = (uint32_t)(ca + cb - 1);
+        scale_consts(L, J.scl, J.scls);
+        CK(cudaMemcpyAsync(s + o_job, &J, sizeof J, cudaMemcpyHostToDevice, st));
+        e = launch_conv_small(g.P3, (const ConvJob *)(s + o_job), 1, (uint32_t)L, !square, st,
+                              8.0 * (double)(na + (square ? 0 : nb)) + 12.0 * (double)J.conv);
+    } else {
+        FourStep G = four_step_geometry(pl, square != 0);
+        FSJob J{};
+        J.a = a, J.b = b, J.na = na, J.nb = nb, J.ca = ca, J.cb = cb;
+        J.ya = ya, J.yb = yb;
+        J.width = w;
+        CK(cudaMemcpyAsync(s + o_job, &J, sizeof J, cudaMemcpyHostToDevice, st));
+        e = launch_four_step(g.P3, G, (const FSJob *)(s + o_job), 1, st, 8.0 * (double)(na + (square ? 0 : nb)));
+    }
+    if (e) return fail(FFG_E_CUDA, "ffg_mul_device_noalloc: %s", cudaGetErrorString(e));
+    CrtJob C{};
+    C.y = ya;
+    C.y_stride = L;
+    C.conv = ca + cb - 1;
+    C.out = out;
+    C.nlimbs = nlimbs;
+    C.width = w;
+    C.nchunks = nchunks;
+    C.add = 0;
+    C.pref = (StepFn *)(s + o_pref);
+    C.cta_fn = (StepFn *)(s + o_fn);
+    C.cta_in = (__int128 *)(s + o_in);
+    e = launch_crt(g.P3, C, st);
+    if (e) return fail(FFG_E_CUDA, "ffg_mul_device_noalloc crt: %s", cudaGetErrorString(e));
+    return FFG_OK;
+}

@@ -72,6 +72,23 @@ int ffg_mul_host(uint64_t *out, size_t *nout, const uint64_t *a, size_t na, cons
 int ffg_mul_device(uint64_t *out, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b, size_t nb,
                    uint64_t bits_b, int square, void *stream);
 
+/* No counterpart in the reference.  ffg_mul_device without any device
+   allocation, for callers that cannot allocate once running: code issuing
+   work while a CUDA graph is being captured, frameworks whose allocator owns
+   all device memory, latency-critical paths that cannot take a cudaMalloc.
+   Scratch comes from one fixed 8 MiB array per GPU, held by every GPU that
+   loads the library until the process exits; products whose scratch does not
+   fit (transform lengths above 2^19 for a square or 2^18 for two distinct
+   operands, about 130 000 and 65 000 limbs per operand), or that need the
+   split multiply, return FFG_E_RANGE with the bytes needed in the message.
+   ffg_init must have run first (it builds the device tables; run it during
+   set-up).  The first call on a device looks the array's address up; make
+   that first call before any stream capture.  All calls share the one array:
+   calls whose GPU work overlaps (different streams, no ordering between
+   them) race and corrupt each other's results. */
+int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b,
+                           size_t nb, uint64_t bits_b, int square, void *stream);
+
 /* fibonacci (src/fib.c:211) from bit i0 down: continues fast doubling from
    the pair (F(k-1), F(k)), k = n >> i0, on the device and returns F(n) as a
    malloc'ed limb array (free with ffg_free).  i0 >= 1. */
