@@ -152,6 +152,72 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_ntt_microbench(args):
+    """One NTT product of --limbs random 64-bit limbs (seeded), square or
+    distinct, repeated: per-family device times and the row pass's fraction of
+    the HBM roofline at that length.  Operands stay on the device."""
+    import numpy as np
+    import torch
+    import fastfib_b200 as ff
+    torch.cuda.set_device(0)
+    ff.set_device(0)
+    ff.init(args.limbs * 2)
+    rng = np.random.default_rng(88172645463325252 % 2**63)
+    n = args.limbs
+    a = rng.integers(0, 2**64, n, dtype=np.uint64)
+    b = rng.integers(0, 2**64, n, dtype=np.uint64)
+    a[-1] |= np.uint64(1 << 63)
+    b[-1] |= np.uint64(1 << 63)
+    da = torch.from_numpy(a.view(np.int64)).cuda()
+    db = torch.from_numpy(b.view(np.int64)).cuda()
+    out = torch.zeros(2 * n + 1, dtype=torch.int64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sq = args.square
+    plan = ff.plan(64 * n, 64 * n, sq)
+
+    def step():
+        ff.mul_device(out.data_ptr(), da.data_ptr(), n, 64 * n, db.data_ptr(), n, 64 * n, sq)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ff.profile(True)
+    t_ms = []
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        torch.cuda.synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+        t_ms.append(e0.elapsed_time(e1))
+    prof = ff.profile_read()
+    ff.profile(False)
+    # check in O(n): the product modulo four 64-bit primes (exact products of
+    # multi-million-limb integers in Python would take minutes)
+    got = out.cpu().numpy().view(np.uint64)
+    x, y = int.from_bytes(a.tobytes(), "little"), int.from_bytes(b.tobytes(), "little")
+    z = int.from_bytes(got.tobytes(), "little")
+    with open(GOLD_FP) as f:
+        primes = [int(p) for p in json.load(f)["primes"]]
+    ok = all(z % p == (x % p) * ((x if sq else y) % p) % p for p in primes) and z.bit_length() <= 128 * n
+    with open(PEAKS) as f:
+        peak = json.load(f)["hbm_gbs"]
+    fam = {k: {"launches": v["launches"], "ms_per_launch": v["ms"] / max(1, v["launches"]),
+               "gbs": v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else 0.0,
+               "frac": (v["bytes"] / (v["ms"] * 1e-3) / 1e9 / peak) if v["ms"] else 0.0}
+           for k, v in prof.items() if v["launches"]}
+    line = {"metric": "NTT multiply ms (microbench)", "value": statistics.mean(t_ms), "unit": "ms",
+            "higher_is_better": False, "steps": args.steps, "warmup": args.warmup, "dtype": "u32",
+            "config": {"workload": f"{'square' if sq else 'product'} of {n}-limb random operands", "plan": plan,
+                       "l2": "flushed before every step"},
+            "bit_exact": ok, "families": fam, "peak_gbs": peak}
+    print(json.dumps(line), flush=True)
+    return 0 if ok else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -161,6 +227,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-f1e9", action="store_true", help="skip the extra F(10^9) measurement")
+    ap.add_argument("--config", default="fib", choices=["fib", "ntt"],
+                    help="fib: F(n) (the headline); ntt: one NTT product of --limbs limbs")
+    ap.add_argument("--limbs", type=int, default=1 << 22)
+    ap.add_argument("--square", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -169,6 +239,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.config == "ntt":
+        return run_ntt_microbench(args)
 
     import torch
     import torch.distributed as dist

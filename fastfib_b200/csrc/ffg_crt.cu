@@ -1,213 +1,273 @@
-// CRT recombination and carry propagation for sm_100a.
+// CRT recombination and the fast-doubling linear passes, for sm_100a.
 //
-// k_crt_chunks: each thread turns 64 consecutive coefficients into exactly
-// `width` limbs.  Per coefficient, Garner's method on the three residues
-//   x2 = (r2 - r1) p1^-1 mod p2,  x3 = ((r3 - r1) p1^-1 - x2) p2^-1 mod p3,
-//   X  = r1 + x2 p1 + x3 p1 p2  < p1 p2 p3 < 2^93,
-// then X is added at bit i*width with a running 128-bit carry (the
-// reference's crt_garner8 / crt_pack64, src/crt.c:38-87).  The CTA stages its
-// 3 x 8192 residues in shared memory (row pad of one word per 64, so the 32
-// threads of a warp reading their own runs hit 32 different banks), writes
-// limbs with carry-in 0 and publishes its chunks' carry maps (ffg_carry.cuh).
-// k_scan_ctas and k_apply_carry then settle the carries between chunks.
-#include "ffg_carry.cuh"
+// k_crt: one CTA per 2048 coefficients (= 32 * width output limbs exactly).
+//   1. Garner's method per coefficient (the reference's crt_garner8,
+//      src/crt.c:38-64), in parallel, for the block plus a halo of the few
+//      coefficients below it that reach into its limbs:
+//        x2 = (r2 - r1) p1^-1 mod p2,  x3 = ((r3 - r1) p1^-1 - x2) p2^-1 mod p3,
+//        X  = r1 + x2 p1 + x3 p1 p2  < p1 p2 p3 < 2^93.
+//   2. Every limb j sums the slices of the coefficients X_i 2^(i b) that
+//      overlap it (3-6 of them): the column sum lo_j + 2^64 hi_j.  This is the
+//      reference's crt_pack64 (src/crt.c:70-87) with the running carry turned
+//      into per-limb sums.
+//   3. cta_resolve (ffg_ripple.cuh) settles the one-bit ripples; k_settle
+//      carries between CTAs.
+// A small signed constant is added to the product on the way (the final
+// +-2 of fast doubling, src/fib.c:249) in two's complement over the output.
+//
+// k_lin: out = alpha s1 + beta s2 + gamma over len limbs, two outputs per
+// launch (the reference's step_proc / last_proc, src/fib.c:37-62, 123-143);
+// negative terms in two's complement (-s = ~s + 1 mod 2^(64 len)), so every
+// column sum is non-negative and the same ripple settle applies.
 #include "ffg_internal.h"
+#include "ffg_ripple.cuh"
 
 namespace ffg {
 
-constexpr uint32_t CRT_COEF = 64 * FFG_CRT_THREADS;          // coefficients per CTA
-constexpr uint32_t CRT_ROW = CRT_COEF + CRT_COEF / 64;       // padded words per prime
+typedef unsigned __int128 u128;
 
-__global__ void __launch_bounds__(FFG_CRT_THREADS) k_crt_chunks(GarnerConst K, CrtJob J) {
-    extern __shared__ uint32_t res[];
-    __shared__ StepFn wt[FFG_CRT_THREADS / 32];
-    const uint64_t gbase = (uint64_t)blockIdx.x * CRT_COEF;
-    for (int k = 0; k < 3; k++) {
-        const uint32_t *y = J.y + (size_t)k * J.y_stride;
-        for (uint32_t i = threadIdx.x; i < CRT_COEF; i += blockDim.x) {
-            uint64_t g = gbase + i;
-            res[k * CRT_ROW + i + (i >> 6)] = g < J.conv ? y[g] : 0;
+constexpr uint32_t CRT_COEF = 2048;     // coefficients per CTA
+constexpr uint32_t CRT_THREADS = 256;
+constexpr uint32_t CRT_HALO_MAX = 24;   // ceil(156 / b) + 1 for b >= 8, rounded up to 4
+constexpr uint32_t CRT_NL_MAX = 32 * 35;
+constexpr uint32_t CRT_NL_PER_W = 32;   // limbs per CTA = 32 * width
+
+FFG_DEV_INLINE int64_t floor_div(int64_t a, int64_t b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+__global__ void __launch_bounds__(CRT_THREADS) k_crt(GarnerConst K, CrtJob J) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    uint64_t *Xlo = (uint64_t *)sm;                              // CRT_COEF + halo
+    uint64_t *lo = Xlo + CRT_COEF + CRT_HALO_MAX;                // NL limbs
+    uint32_t *Xhi = (uint32_t *)(lo + CRT_NL_MAX);               // CRT_COEF + halo
+    uint32_t *hi = Xhi + CRT_COEF + CRT_HALO_MAX;                // NL
+    uint32_t *gG = hi + CRT_NL_MAX, *gP = gG + CRT_NL_MAX / 32, *gin = gP + CRT_NL_MAX / 32;
+    __shared__ uint32_t hiprev_s;
+
+    const uint32_t b = J.width, NL = CRT_NL_PER_W * b;
+    const int32_t halo = (int32_t)(((156 + b - 1) / b + 1 + 3) & ~3u);
+    const int64_t ibase = (int64_t)blockIdx.x * CRT_COEF;
+    const uint32_t p1 = K.p[0], p2 = K.p[1], p3 = K.p[2];
+
+    // residues in 16-byte vectors of 4 coefficients, every load of the thread
+    // issued before any arithmetic (ibase - halo and the strides are multiples
+    // of 4, and every residue array is a multiple of 16 words long)
+    constexpr int VPT = (CRT_COEF + CRT_HALO_MAX) / 4 / CRT_THREADS + 1; // vectors per thread
+    const int32_t nvec = ((int32_t)CRT_COEF + halo) / 4;
+    uint4 rv[VPT][3];
+#pragma unroll
+    for (int v = 0; v < VPT; v++) {
+        const int32_t t4 = (int32_t)threadIdx.x + v * (int32_t)blockDim.x;
+        const int64_t gi = ibase - halo + 4 * (int64_t)t4;
+        const bool in = t4 < nvec && gi >= 0 && (uint64_t)gi < J.conv;
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            rv[v][k] = in ? __ldg((const uint4 *)(J.y + k * J.y_stride + gi)) : make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int v = 0; v < VPT; v++) {
+        const int32_t t4 = (int32_t)threadIdx.x + v * (int32_t)blockDim.x;
+        if (t4 >= nvec) break;
+        const int64_t gi0 = ibase - halo + 4 * (int64_t)t4;
+        const uint32_t r1s[4] = {rv[v][0].x, rv[v][0].y, rv[v][0].z, rv[v][0].w};
+        const uint32_t r2s[4] = {rv[v][1].x, rv[v][1].y, rv[v][1].z, rv[v][1].w};
+        const uint32_t r3s[4] = {rv[v][2].x, rv[v][2].y, rv[v][2].z, rv[v][2].w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int64_t gi = gi0 + e;
+            u128 X = 0;
+            if (gi >= 0 && (uint64_t)gi < J.conv) {
+                const uint32_t r1 = r1s[e], r2 = r2s[e], r3 = r3s[e];
+                const uint32_t x1m2 = min(r1, r1 - p2);
+                const uint32_t x2 = shoup(r2 - x1m2 + p2, K.i12, K.i12s, p2);
+                const uint32_t x1m3 = min(r1, r1 - p3);
+                const uint32_t t3 = shoup(r3 - x1m3 + p3, K.i13, K.i13s, p3);
+                const uint32_t x2m3 = min(x2, x2 - p3);
+                const uint32_t x3 = shoup(t3 - x2m3 + p3, K.i23, K.i23s, p3);
+                X = (u128)((uint64_t)x2 * p1 + r1) + (u128)x3 * K.p12;
+            }
+            Xlo[4 * t4 + e] = (uint64_t)X;
+            Xhi[4 * t4 + e] = (uint32_t)(X >> 64);
         }
     }
     __syncthreads();
 
-    const uint32_t t = threadIdx.x;
-    const uint64_t chunk = (uint64_t)blockIdx.x * FFG_CRT_THREADS + t;
-    StepFn f = const_fn(0);
-    if (chunk < J.nchunks) {
-        const uint32_t b = J.width, p1 = K.p[0], p2 = K.p[1], p3 = K.p[2];
-        const uint64_t mask = (1ull << b) - 1;
-        const uint64_t start = chunk * b;
-        const uint64_t lim = J.nlimbs - start; // limbs of this chunk inside the output
-        uint64_t *out = J.out + start;
-        u128 carry = 0, buf = 0;
-        uint32_t nbits = 0, e = 0;
-        uint64_t l0 = 0, l1 = 0;
-        bool ones = true, zero = true;
-        const uint32_t *r = res + 65 * t;
-        for (int k = 0; k < 64; k++) {
-            uint32_t r1 = r[k], r2 = r[CRT_ROW + k], r3 = r[2 * CRT_ROW + k];
-            uint32_t x1m2 = min(r1, r1 - p2);
-            uint32_t x2 = shoup(r2 - x1m2 + p2, K.i12, K.i12s, p2);
-            uint32_t x1m3 = min(r1, r1 - p3);
-            uint32_t t3 = shoup(r3 - x1m3 + p3, K.i13, K.i13s, p3);
-            uint32_t x2m3 = min(x2, x2 - p3);
-            uint32_t x3 = shoup(t3 - x2m3 + p3, K.i23, K.i23s, p3);
-            u128 X = (u128)((uint64_t)x2 * p1 + r1) + (u128)x3 * K.p12;
-            u128 acc = X + carry;
-            uint64_t v = (uint64_t)acc & mask;
-            carry = acc >> b;
-            buf |= (u128)v << nbits;
-            nbits += b;
-            if (nbits >= 64) {
-                uint64_t limb = (uint64_t)buf;
-                buf >>= 64;
-                nbits -= 64;
-                if (e < lim) out[e] = limb;
-                if (e == 0) l0 = limb;
-                else if (e == 1) l1 = limb;
-                else {
-                    ones &= limb == ~0ull;
-                    zero &= limb == 0;
-                }
-                e++;
-            }
+    // column sums; j = -1 (the limb below the CTA) only for its high part
+    const uint64_t j0 = (uint64_t)blockIdx.x * NL;
+    const bool neg_add = J.add < 0;
+    for (int32_t j = (int32_t)threadIdx.x - 1; j < (int32_t)NL; j += blockDim.x) {
+        const int64_t ilo = floor_div(64 * (int64_t)j - 92 + b - 1, b), ihi = floor_div(64 * (int64_t)j + 63, b);
+        uint64_t s_lo = 0;
+        uint32_t s_hi = 0;
+        for (int64_t i = ilo < -halo ? -halo : ilo; i <= ihi; i++) {
+            const u128 X = ((u128)Xhi[i + halo] << 64) | Xlo[i + halo];
+            const int64_t s = i * (int64_t)b - 64 * (int64_t)j;
+            const uint64_t part = s >= 0 ? (uint64_t)(X << s) : (uint64_t)(X >> (-s));
+            s_lo += part;
+            s_hi += s_lo < part;
         }
-        f = chunk_fn((i128)carry, ((u128)l1 << 64) | l0, ones, zero);
+        // the constant: +add at limb 0, or 2^(64 nlimbs) + add when negative
+        const int64_t jabs = (int64_t)j0 + j;
+        if (J.add != 0 && jabs >= 0 && (uint64_t)jabs < J.nlimbs) {
+            const uint64_t c = jabs == 0 ? (uint64_t)J.add : (neg_add ? ~0ull : 0ull);
+            s_lo += c;
+            s_hi += s_lo < c;
+        }
+        if (j < 0) hiprev_s = s_hi;
+        else {
+            lo[j] = s_lo;
+            hi[j] = s_hi;
+        }
     }
-    StepFn I = cta_scan(f, wt);
-    if (chunk < J.nchunks) J.pref[chunk] = I;
-    if (t == blockDim.x - 1) J.cta_fn[blockIdx.x] = I;
+    __syncthreads();
+    const uint32_t map = cta_resolve(lo, hi, blockIdx.x ? hiprev_s : 0, NL, gG, gP, gin);
+    for (uint32_t j = threadIdx.x; j < NL && j0 + j < J.nlimbs; j += blockDim.x) J.out[j0 + j] = lo[j];
+    if (threadIdx.x == 0) J.maps[blockIdx.x] = map;
 }
 
-// One warp: the carry into every CTA from the CTAs' maps and the carry into
-// the first one.  Lane l composes a contiguous run of maps, the lanes scan
-// their runs, then each lane walks its run once more writing carries.
-__global__ void __launch_bounds__(32) k_scan_ctas(const StepFn *__restrict__ fn, uint32_t n, int64_t c0,
-                                                  __int128 *__restrict__ cin) {
-    const uint32_t lane = threadIdx.x;
-    const uint32_t seg = (n + 31) / 32, s0 = min(n, lane * seg), s1 = min(n, s0 + seg);
-    StepFn F = const_fn(0);
-    if (s0 < s1) {
-        F = fn[s0];
-        for (uint32_t k = s0 + 1; k < s1; k++) F = fn_then(F, fn[k]);
+// Carries between CTAs: one warp per 32 CTAs composes the maps of every CTA
+// before them (from carry 0 into the first), then each lane whose CTA
+// receives a carry adds it into that CTA's lowest limbs.
+__global__ void __launch_bounds__(32) k_settle(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs,
+                                               const uint32_t *__restrict__ maps, uint32_t ncta) {
+    const uint32_t lane = threadIdx.x, first = blockIdx.x * 32;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < first; base += 32) {
+        const uint32_t m = maps[base + lane]; // base + 32 <= first <= ncta
+        const uint32_t inc = warp_map_scan(m);
+        carry = map_apply(__shfl_sync(0xffffffffu, inc, 31), carry);
     }
-    // inclusive scan over lanes (empty runs only at the tail, never read)
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        StepFn G = shfl_up_fn(F, d);
-        if ((int)lane >= d) F = fn_then(G, F);
-    }
-    StepFn prev = shfl_up_fn(F, 1);
-    i128 c = lane == 0 ? (i128)c0 : fn_apply(prev, (i128)c0);
-    for (uint32_t k = s0; k < s1; k++) {
-        cin[k] = c;
-        c = fn_apply(fn[k], c);
+    const uint32_t q = first + lane;
+    const uint32_t m = q < ncta ? maps[q] : 2u;
+    const uint32_t inc = warp_map_scan(m);
+    uint32_t exc = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) exc = 2u;
+    const uint32_t c = map_apply(exc, carry);
+    if (q < ncta && c) {
+        const uint64_t end = min(nlimbs, (uint64_t)(q + 1) * cta_limbs);
+        for (uint64_t j = (uint64_t)q * cta_limbs; j < end; j++)
+            if (++out[j] != 0) break;
     }
 }
 
-// Adds each chunk's carry-in (from its CTA's carry-in and the stored prefix
-// map of the chunks before it) into its lowest limbs.
-__global__ void __launch_bounds__(256) k_apply_carry(uint64_t *out, uint64_t nlimbs, uint32_t chunk_limbs,
-                                                     uint32_t nchunks, uint32_t cta_chunks,
-                                                     const StepFn *__restrict__ pref,
-                                                     const __int128 *__restrict__ cta_in) {
-    const uint64_t chunk = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (chunk >= nchunks) return;
-    const uint64_t cta = chunk / cta_chunks;
-    i128 c = cta_in[cta];
-    if (chunk % cta_chunks) c = fn_apply(pref[chunk - 1], c);
-    const uint64_t start = chunk * chunk_limbs;
-    const uint64_t n = min((uint64_t)chunk_limbs, nlimbs - start);
-    add_carry_in(out + start, n, c);
-}
-
-cudaError_t launch_scan_apply(uint64_t *out, uint64_t nlimbs, uint32_t chunk_limbs, uint32_t nchunks,
-                              uint32_t cta_chunks, const StepFn *pref, const StepFn *cta_fn, __int128 *cta_in,
-                              int64_t c0, cudaStream_t st) {
-    const uint32_t ncta = (nchunks + cta_chunks - 1) / cta_chunks;
-    prof_begin(PK_CARRY, st);
-    k_scan_ctas<<<1, 32, 0, st>>>(cta_fn, ncta, c0, cta_in);
-    cudaError_t e = cudaGetLastError();
-    if (e) return e;
-    k_apply_carry<<<(nchunks + 255) / 256, 256, 0, st>>>(out, nlimbs, chunk_limbs, nchunks, cta_chunks, pref, cta_in);
-    prof_end(PK_CARRY, st, (double)nchunks * (sizeof(StepFn) + 32));
+static cudaError_t launch_settle(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *maps,
+                                 uint32_t ncta, cudaStream_t st) {
+    if (ncta <= 1) return cudaSuccess; // nothing comes into the first CTA
+    k_settle<<<(ncta + 31) / 32, 32, 0, st>>>(out, nlimbs, cta_limbs, maps, ncta);
     return cudaGetLastError();
+}
+
+uint32_t crt_ctas(uint64_t nlimbs, uint32_t width) {
+    const uint64_t NL = (uint64_t)CRT_NL_PER_W * width;
+    return (uint32_t)((nlimbs + NL - 1) / NL);
+}
+
+static size_t crt_smem() {
+    return (CRT_COEF + CRT_HALO_MAX) * (8 + 4) + CRT_NL_MAX * (8 + 4) + 3 * (CRT_NL_MAX / 32) * 4;
 }
 
 cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st) {
     (void)P3;
     static bool configured = false;
-    const size_t sm = 3 * CRT_ROW * sizeof(uint32_t);
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_crt_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = cudaFuncSetAttribute(k_crt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)crt_smem());
         if (e) return e;
         configured = true;
     }
-    const uint32_t ncta = (J.nchunks + FFG_CRT_THREADS - 1) / FFG_CRT_THREADS;
+    const uint32_t ncta = crt_ctas(J.nlimbs, J.width);
     prof_begin(PK_CRT, st);
-    k_crt_chunks<<<ncta, FFG_CRT_THREADS, sm, st>>>(garner_const(), J);
+    k_crt<<<ncta, CRT_THREADS, crt_smem(), st>>>(garner_const(), J);
     prof_end(PK_CRT, st, 12.0 * (double)J.conv + 8.0 * (double)J.nlimbs);
     cudaError_t e = cudaGetLastError();
     if (e) return e;
-    return launch_scan_apply(J.out, J.nlimbs, J.width, J.nchunks, FFG_CRT_THREADS, J.pref, J.cta_fn, J.cta_in,
-                             J.add, st);
+    prof_begin(PK_CARRY, st);
+    e = launch_settle(J.out, J.nlimbs, CRT_NL_PER_W * J.width, J.maps, ncta, st);
+    prof_end(PK_CARRY, st, 4.0 * ncta);
+    return e;
 }
 
 // ------------------------------------------------------------ linear passes
 
-// out_k = alpha_k s1 + beta_k s2 (+ gamma_k, fed in as the first carry) over
-// len limbs, FFG_LIN_K limbs per thread: the reference's step_proc and
-// last_proc (src/fib.c:37-62, 123-143) with parallel carries.
-__global__ void __launch_bounds__(FFG_LIN_THREADS) k_lin_chunks(LinJob J) {
-    __shared__ StepFn wt[FFG_LIN_THREADS / 32];
-    const uint64_t chunk = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t start = chunk * FFG_LIN_K;
-    const uint32_t ncta = gridDim.x;
-    for (uint32_t k = 0; k < J.nout; k++) {
-        StepFn f = const_fn(0);
-        if (chunk < J.nchunks) {
-            const i128 al = J.alpha[k], be = J.beta[k];
-            uint64_t *o = J.out[k];
-            i128 c = 0;
-            uint64_t l0 = 0, l1 = 0;
-            bool ones = true, zero = true;
+constexpr uint32_t LIN_NL = 2048; // limbs per CTA
+constexpr uint32_t LIN_THREADS = 256;
+
+uint32_t lin_ctas(uint64_t len) { return (uint32_t)((len + LIN_NL - 1) / LIN_NL); }
+
+// Column sum of output k at limb j (0 past the output), from the limbs x, y
+// of s1, s2 at j.
+FFG_DEV_INLINE void lin_colsum(const LinJob &J, uint32_t k, uint64_t j, uint64_t x, uint64_t y, uint64_t &s_lo,
+                               uint32_t &s_hi) {
+    s_lo = 0;
+    s_hi = 0;
+    if (j >= J.len) return;
+    const int64_t al = k ? J.alpha[1] : J.alpha[0], be = k ? J.beta[1] : J.beta[0];
+    const int64_t ga = k ? J.gamma[1] : J.gamma[0];
+    const u128 t = (u128)(al >= 0 ? x : ~x) * (uint64_t)(al >= 0 ? al : -al) +
+                   (u128)(be >= 0 ? y : ~y) * (uint64_t)(be >= 0 ? be : -be);
+    // constant: gamma plus one per negative term (-s = ~s + 1), two's complement
+    const int64_t c = ga + (al < 0 ? -al : 0) + (be < 0 ? -be : 0);
+    const uint64_t cj = j == 0 ? (uint64_t)c : (c < 0 ? ~0ull : 0ull);
+    const u128 sum = t + cj;
+    s_lo = (uint64_t)sum;
+    s_hi = (uint32_t)(sum >> 64);
+}
+
+__global__ void __launch_bounds__(LIN_THREADS) k_lin(LinJob J) {
+    __shared__ uint64_t lo[LIN_NL];
+    __shared__ uint32_t hi[LIN_NL];
+    __shared__ uint32_t gG[LIN_NL / 32], gP[LIN_NL / 32], gin[LIN_NL / 32];
+    __shared__ uint32_t hiprev_s;
+    constexpr int PER = LIN_NL / LIN_THREADS;
+    const uint64_t j0 = (uint64_t)blockIdx.x * LIN_NL;
+    // every limb this thread needs, loaded once for both outputs
+    uint64_t xs[PER], ys[PER];
 #pragma unroll
-            for (uint32_t i = 0; i < FFG_LIN_K; i++) {
-                const uint64_t idx = start + i;
-                const uint64_t x = idx < J.n1 ? J.s1[idx] : 0, y = idx < J.n2 ? J.s2[idx] : 0;
-                i128 v = al * (i128)x + be * (i128)y + c;
-                const uint64_t limb = (uint64_t)v;
-                c = v >> 64;
-                if (idx < J.len) o[idx] = limb;
-                if (i == 0) l0 = limb;
-                else if (i == 1) l1 = limb;
-                else {
-                    ones &= limb == ~0ull;
-                    zero &= limb == 0;
-                }
-            }
-            f = chunk_fn(c, ((u128)l1 << 64) | l0, ones, zero);
+    for (int r = 0; r < PER; r++) {
+        const uint64_t j = j0 + threadIdx.x + r * LIN_THREADS;
+        xs[r] = j < J.n1 ? __ldg(&J.s1[j]) : 0;
+        ys[r] = j < J.n2 ? __ldg(&J.s2[j]) : 0;
+    }
+    uint64_t xp = 0, yp = 0; // limb j0 - 1, for the carry into the CTA's first limb
+    if (threadIdx.x == 0 && j0 > 0) {
+        xp = j0 - 1 < J.n1 ? J.s1[j0 - 1] : 0;
+        yp = j0 - 1 < J.n2 ? J.s2[j0 - 1] : 0;
+    }
+    for (uint32_t k = 0; k < J.nout; k++) {
+#pragma unroll
+        for (int r = 0; r < PER; r++) {
+            const uint32_t jl = threadIdx.x + r * LIN_THREADS;
+            uint64_t s_lo;
+            uint32_t s_hi;
+            lin_colsum(J, k, j0 + jl, xs[r], ys[r], s_lo, s_hi);
+            lo[jl] = s_lo;
+            hi[jl] = s_hi;
         }
-        StepFn I = cta_scan(f, wt);
-        if (chunk < J.nchunks) J.pref[(size_t)k * J.nchunks + chunk] = I;
-        if (threadIdx.x == blockDim.x - 1) J.cta_fn[(size_t)k * ncta + blockIdx.x] = I;
+        if (threadIdx.x == 0) {
+            uint64_t s_lo = 0;
+            uint32_t s_hi = 0;
+            if (j0 > 0) lin_colsum(J, k, j0 - 1, xp, yp, s_lo, s_hi);
+            hiprev_s = s_hi;
+        }
+        __syncthreads();
+        const uint32_t map = cta_resolve(lo, hi, hiprev_s, LIN_NL, gG, gP, gin);
+        uint64_t *o = k ? J.out[1] : J.out[0];
+        for (uint32_t j = threadIdx.x; j < LIN_NL && j0 + j < J.len; j += blockDim.x) o[j0 + j] = lo[j];
+        if (threadIdx.x == 0) J.maps[(size_t)k * gridDim.x + blockIdx.x] = map;
+        __syncthreads();
     }
 }
 
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st) {
-    const uint32_t ncta = (J.nchunks + FFG_LIN_THREADS - 1) / FFG_LIN_THREADS;
+    const uint32_t ncta = lin_ctas(J.len);
     prof_begin(PK_LIN, st);
-    k_lin_chunks<<<ncta, FFG_LIN_THREADS, 0, st>>>(J);
+    k_lin<<<ncta, LIN_THREADS, 0, st>>>(J);
     prof_end(PK_LIN, st, 8.0 * (double)(J.n1 + J.n2) + 8.0 * (double)J.len * J.nout);
     cudaError_t e = cudaGetLastError();
     if (e) return e;
-    for (uint32_t k = 0; k < J.nout; k++) {
-        e = launch_scan_apply(J.out[k], J.len, FFG_LIN_K, J.nchunks, FFG_LIN_THREADS, J.pref + (size_t)k * J.nchunks,
-                              J.cta_fn + (size_t)k * ncta, J.cta_in + (size_t)k * ncta, J.gamma[k], st);
-        if (e) return e;
-    }
-    return cudaSuccess;
+    prof_begin(PK_CARRY, st);
+    for (uint32_t k = 0; k < J.nout && !e; k++)
+        e = launch_settle(J.out[k], J.len, LIN_NL, J.maps + (size_t)k * ncta, ncta, st);
+    prof_end(PK_CARRY, st, 4.0 * ncta * J.nout);
+    return e;
 }
 
 } // namespace ffg

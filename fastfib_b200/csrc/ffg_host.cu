@@ -389,7 +389,7 @@ static FourStep four_step_geometry(const ffg_plan &pl, bool square) {
     G.rn = pl.lg - G.c;
     G.r3 = pl.r3;
     G.R = (pl.r3 ? 3u : 1u) << G.rn;
-    uint32_t wc = 32768u / G.R;
+    uint32_t wc = 16384u / G.R; // a column tile of about 64 KB of shared memory
     wc = wc < 8 ? 8 : (wc > 64 ? 64 : wc);
     while (wc & (wc - 1)) wc &= wc - 1;
     if (wc > (1u << G.c)) wc = 1u << G.c;
@@ -417,9 +417,12 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
     }
     const uint32_t w = pl.width;
     cudaError_t e = cudaSuccess;
+    double bytes = 0;
+    if (count > FFG_CONV_JOBS) return fail(FFG_E_ARG, "%d products in one launch", count);
     if (pl.kernel == 0) {
+        ConvJobs jobs{};
         for (int i = 0; i < count; i++) {
-            ConvJob J{};
+            ConvJob &J = jobs.j[i];
             J.a = pr[i].a, J.b = square ? pr[i].a : pr[i].b;
             J.na = pr[i].na, J.nb = square ? pr[i].na : pr[i].nb;
             J.ca = (pr[i].bits_a + w - 1) / w;
@@ -431,17 +434,15 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
             J.conv = (uint32_t)(J.ca + J.cb - 1);
             memcpy(J.scl, scl, sizeof scl);
             memcpy(J.scls, scls, sizeof scls);
-            ALLOC(dj, ConvJob, 1);
-            CK(cudaMemcpyAsync(dj, &J, sizeof J, cudaMemcpyHostToDevice, st));
-            e = launch_conv_small(g.P3, dj, 1, (uint32_t)L, !square, st,
-                                  8.0 * (double)(J.na + (square ? 0 : J.nb)) + 12.0 * (double)J.conv);
-            if (e) return fail(FFG_E_CUDA, "conv_small: %s", cudaGetErrorString(e));
+            bytes += 8.0 * (double)(J.na + (square ? 0 : J.nb)) + 12.0 * (double)J.conv;
         }
+        e = launch_conv_small(g.P3, jobs, (uint32_t)count, (uint32_t)L, !square, st, bytes);
+        if (e) return fail(FFG_E_CUDA, "conv_small: %s", cudaGetErrorString(e));
     } else {
         FourStep G = four_step_geometry(pl, square);
-        std::vector<FSJob> jobs(count);
+        FSJobs jobs{};
         for (int i = 0; i < count; i++) {
-            FSJob &J = jobs[i];
+            FSJob &J = jobs.j[i];
             J.a = pr[i].a, J.b = square ? pr[i].a : pr[i].b;
             J.na = pr[i].na, J.nb = square ? pr[i].na : pr[i].nb;
             J.ca = (pr[i].bits_a + w - 1) / w;
@@ -449,11 +450,9 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
             J.ya = ya[i], J.yb = yb[i];
             J.width = w;
         }
-        ALLOC(dj, FSJob, count);
-        CK(cudaMemcpyAsync(dj, jobs.data(), count * sizeof(FSJob), cudaMemcpyHostToDevice, st));
         double limb_bytes = 0;
-        for (int i = 0; i < count; i++) limb_bytes += 8.0 * (double)(jobs[i].na + (square ? 0 : jobs[i].nb));
-        e = launch_four_step(g.P3, G, dj, (uint32_t)count, st, limb_bytes);
+        for (int i = 0; i < count; i++) limb_bytes += 8.0 * (double)(jobs.j[i].na + (square ? 0 : jobs.j[i].nb));
+        e = launch_four_step(g.P3, G, jobs, (uint32_t)count, st, limb_bytes);
         if (e) return fail(FFG_E_CUDA, "four_step: %s", cudaGetErrorString(e));
     }
     for (int i = 0; i < count; i++) {
@@ -465,13 +464,9 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
         C.out = pr[i].out;
         C.nlimbs = pr[i].na + (square ? pr[i].na : pr[i].nb) + 1;
         C.width = w;
-        C.nchunks = (uint32_t)((C.nlimbs + w - 1) / w);
         C.add = pr[i].add;
-        uint32_t ncta = (C.nchunks + FFG_CRT_THREADS - 1) / FFG_CRT_THREADS;
-        C.pref = (StepFn *)arena_alloc((size_t)C.nchunks * sizeof(StepFn));
-        C.cta_fn = (StepFn *)arena_alloc((size_t)ncta * sizeof(StepFn));
-        C.cta_in = (__int128 *)arena_alloc((size_t)ncta * sizeof(__int128));
-        if (!C.pref || !C.cta_fn || !C.cta_in) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
+        C.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(C.nlimbs, w) * sizeof(uint32_t));
+        if (!C.maps) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
         e = launch_crt(g.P3, C, st);
         if (e) return fail(FFG_E_CUDA, "crt: %s", cudaGetErrorString(e));
     }
@@ -522,13 +517,22 @@ static int run_split(const Prod &pr, bool square, const ffg_plan &pl, cudaStream
         J.acc_stride = Lyst;
         J.width = w;
     }
-    ALLOC(dj, FSJob, jobs.size());
-    CK(cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(FSJob), cudaMemcpyHostToDevice, st));
-    cudaError_t e = launch_split_forward(g.P3, G, dj, (uint32_t)np, st, limb_bytes);
-    if (e) return fail(FFG_E_CUDA, "split forward: %s", cudaGetErrorString(e));
+    cudaError_t e = cudaSuccess;
+    for (uint64_t f = 0; f < np; f += FFG_FS_JOBS) {
+        FSJobs part{};
+        const uint64_t cnt = std::min<uint64_t>(FFG_FS_JOBS, np - f);
+        double lb = 0;
+        for (uint64_t k = 0; k < cnt; k++) {
+            part.j[k] = jobs[f + k];
+            lb += (double)jobs[f + k].ca * w / 8.0;
+        }
+        e = launch_split_forward(g.P3, G, part, (uint32_t)cnt, st, lb);
+        if (e) return fail(FFG_E_CUDA, "split forward: %s", cudaGetErrorString(e));
+    }
+    (void)limb_bytes;
     for (uint64_t m = 0; m < nm; m++) {
         const uint64_t i0 = m + 1 > kb ? m + 1 - kb : 0, i1 = std::min(m, ka - 1);
-        e = launch_split_piece(g.P3, G, dj + np + m, (uint32_t)(i1 - i0 + 1), st);
+        e = launch_split_piece(g.P3, G, jobs[np + m], (uint32_t)(i1 - i0 + 1), st);
         if (e) return fail(FFG_E_CUDA, "split piece %llu: %s", (unsigned long long)m, cudaGetErrorString(e));
     }
     CrtJob C{};
@@ -538,13 +542,9 @@ static int run_split(const Prod &pr, bool square, const ffg_plan &pl, cudaStream
     C.out = pr.out;
     C.nlimbs = pr.na + (square ? pr.na : pr.nb) + 1;
     C.width = w;
-    C.nchunks = (uint32_t)((C.nlimbs + w - 1) / w);
     C.add = pr.add;
-    const uint32_t ncta = (C.nchunks + FFG_CRT_THREADS - 1) / FFG_CRT_THREADS;
-    C.pref = (StepFn *)arena_alloc((size_t)C.nchunks * sizeof(StepFn));
-    C.cta_fn = (StepFn *)arena_alloc((size_t)ncta * sizeof(StepFn));
-    C.cta_in = (__int128 *)arena_alloc((size_t)ncta * sizeof(__int128));
-    if (!C.pref || !C.cta_fn || !C.cta_in) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
+    C.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(C.nlimbs, w) * sizeof(uint32_t));
+    if (!C.maps) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
     e = launch_crt(g.P3, C, st);
     if (e) return fail(FFG_E_CUDA, "crt: %s", cudaGetErrorString(e));
     return FFG_OK;
@@ -595,12 +595,8 @@ static int lin(const uint64_t *s1, uint64_t n1, const uint64_t *s2, uint64_t n2,
     J.alpha[0] = a0, J.beta[0] = b0, J.gamma[0] = g0;
     J.alpha[1] = a1, J.beta[1] = b1, J.gamma[1] = g1;
     J.nout = (uint32_t)nout;
-    J.nchunks = (uint32_t)((len + FFG_LIN_K - 1) / FFG_LIN_K);
-    uint32_t ncta = (J.nchunks + FFG_LIN_THREADS - 1) / FFG_LIN_THREADS;
-    J.pref = (StepFn *)arena_alloc(2 * (size_t)J.nchunks * sizeof(StepFn));
-    J.cta_fn = (StepFn *)arena_alloc(2 * (size_t)ncta * sizeof(StepFn));
-    J.cta_in = (__int128 *)arena_alloc(2 * (size_t)ncta * sizeof(__int128));
-    if (!J.pref || !J.cta_fn || !J.cta_in) return fail(FFG_E_NOMEM, "device arena: linear pass scratch");
+    J.maps = (uint32_t *)arena_alloc(2 * (size_t)lin_ctas(len) * sizeof(uint32_t));
+    if (!J.maps) return fail(FFG_E_NOMEM, "device arena: linear pass scratch");
     cudaError_t e = launch_lin(J, st);
     if (e) return fail(FFG_E_CUDA, "linear pass: %s", cudaGetErrorString(e));
     return FFG_OK;
@@ -921,18 +917,13 @@ extern "C" int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t n
     if (rc) return rc;
     if (pl.split) return fail(FFG_E_RANGE, "ffg_mul_device_noalloc: the product needs the split multiply");
 
-    // scratch layout: job record | residues of a | residues of b | CRT carry maps
+    // scratch layout: residues of a | residues of b | CRT carry maps
     const uint64_t L = pl.L;
     const uint32_t w = pl.width;
-    const uint32_t nchunks = (uint32_t)((nlimbs + w - 1) / w);
-    const uint32_t ncta = (nchunks + FFG_CRT_THREADS - 1) / FFG_CRT_THREADS;
-    const size_t o_job = 0;
-    const size_t o_ya = o_job + up256(std::max(sizeof(ConvJob), sizeof(FSJob)));
+    const size_t o_ya = 0;
     const size_t o_yb = o_ya + up256(3 * L * sizeof(uint32_t));
-    const size_t o_pref = o_yb + (square ? 0 : up256(3 * L * sizeof(uint32_t)));
-    const size_t o_fn = o_pref + up256((size_t)nchunks * sizeof(StepFn));
-    const size_t o_in = o_fn + up256((size_t)ncta * sizeof(StepFn));
-    const size_t need = o_in + up256((size_t)ncta * sizeof(__int128));
+    const size_t o_maps = o_yb + (square ? 0 : up256(3 * L * sizeof(uint32_t)));
+    const size_t need = o_maps + up256((size_t)crt_ctas(nlimbs, w) * sizeof(uint32_t));
     if (need > kNoAllocBytes)
         return fail(FFG_E_RANGE,
                     "ffg_mul_device_noalloc: %llu x %llu bits needs %zu bytes of scratch, the limit is %zu bytes",
@@ -942,7 +933,8 @@ extern "C" int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t n
     const uint64_t ca = (bits_a + w - 1) / w, cb = (bits_b + w - 1) / w;
     cudaError_t e;
     if (pl.kernel == 0) {
-        ConvJob J{};
+        ConvJobs jobs{};
+        ConvJob &J = jobs.j[0];
         J.a = a, J.b = b, J.na = na, J.nb = nb, J.ca = ca, J.cb = cb;
         J.y = ya;
         J.y_stride = L;
@@ -950,17 +942,16 @@ extern "C" int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t n
         J.n = pl.lg, J.r3 = pl.r3, J.width = w, J.square = square != 0;
         J.conv = (uint32_t)(ca + cb - 1);
         scale_consts(L, J.scl, J.scls);
-        CK(cudaMemcpyAsync(s + o_job, &J, sizeof J, cudaMemcpyHostToDevice, st));
-        e = launch_conv_small(g.P3, (const ConvJob *)(s + o_job), 1, (uint32_t)L, !square, st,
+        e = launch_conv_small(g.P3, jobs, 1, (uint32_t)L, !square, st,
                               8.0 * (double)(na + (square ? 0 : nb)) + 12.0 * (double)J.conv);
     } else {
         FourStep G = four_step_geometry(pl, square != 0);
-        FSJob J{};
+        FSJobs jobs{};
+        FSJob &J = jobs.j[0];
         J.a = a, J.b = b, J.na = na, J.nb = nb, J.ca = ca, J.cb = cb;
         J.ya = ya, J.yb = yb;
         J.width = w;
-        CK(cudaMemcpyAsync(s + o_job, &J, sizeof J, cudaMemcpyHostToDevice, st));
-        e = launch_four_step(g.P3, G, (const FSJob *)(s + o_job), 1, st, 8.0 * (double)(na + (square ? 0 : nb)));
+        e = launch_four_step(g.P3, G, jobs, 1, st, 8.0 * (double)(na + (square ? 0 : nb)));
     }
     if (e) return fail(FFG_E_CUDA, "ffg_mul_device_noalloc: %s", cudaGetErrorString(e));
     CrtJob C{};
@@ -970,11 +961,8 @@ extern "C" int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t n
     C.out = out;
     C.nlimbs = nlimbs;
     C.width = w;
-    C.nchunks = nchunks;
     C.add = 0;
-    C.pref = (StepFn *)(s + o_pref);
-    C.cta_fn = (StepFn *)(s + o_fn);
-    C.cta_in = (__int128 *)(s + o_in);
+    C.maps = (uint32_t *)(s + o_maps);
     e = launch_crt(g.P3, C, st);
     if (e) return fail(FFG_E_CUDA, "ffg_mul_device_noalloc crt: %s", cudaGetErrorString(e));
     return FFG_OK;

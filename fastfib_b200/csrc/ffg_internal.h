@@ -69,15 +69,8 @@ struct FSJob {
     uint64_t acc_off, acc_stride;
 };
 
-// A chunk's (or a run of chunks') carry map c_in -> c_out: a step function
-// with at most three values (see ffg_carry.cuh).
-struct StepFn {
-    __int128 tlo, thi;       // c < tlo -> va; tlo <= c < thi -> vb; c >= thi -> vc
-    __int128 va, vb, vc;
-};
-
 // The CRT of one product: residues (3 arrays of y_stride words, natural
-// order) -> nlimbs limbs at out, plus `add` (a small signed constant) at limb 0.
+// order) -> nlimbs limbs at out, plus `add` (a small signed constant).
 struct CrtJob {
     const uint32_t *y;
     uint64_t y_stride;
@@ -85,11 +78,9 @@ struct CrtJob {
     uint64_t *out;
     uint64_t nlimbs;
     uint32_t width;
-    uint32_t nchunks;        // ceil(nlimbs / width): 64 coefficients each
+    uint32_t pad;
     int64_t add;
-    StepFn *pref;            // per chunk: the map of chunks [CTA start, chunk]
-    StepFn *cta_fn;          // one per CTA
-    __int128 *cta_in;        // carry into each CTA
+    uint32_t *maps;          // crt_ctas(nlimbs, width) words: each CTA's carry map
 };
 
 // A linear combination out_k = alpha_k s1 + beta_k s2 + gamma_k over len limbs
@@ -101,23 +92,32 @@ struct LinJob {
     int32_t alpha[2], beta[2];
     int64_t gamma[2];
     uint32_t nout;
-    uint32_t nchunks;        // ceil(len / FFG_LIN_K)
-    StepFn *pref;            // 2 * nchunks: per output, as CrtJob::pref
-    StepFn *cta_fn;          // 2 per CTA
-    __int128 *cta_in;        // 2 per CTA
+    uint32_t pad;
+    uint32_t *maps;          // 2 * lin_ctas(len) words: each CTA's carry map per output
 };
 
-constexpr uint32_t FFG_CRT_THREADS = 128; // chunks (of 64 coefficients) per CTA
-constexpr uint32_t FFG_LIN_K = 8;         // limbs per thread in the linear kernels
-constexpr uint32_t FFG_LIN_THREADS = 256;
+// Jobs travel to the kernels by value, as kernel parameters: nothing is
+// copied to the device per launch, so launches queue up without waiting and
+// a whole chain can be captured into a CUDA graph.
+constexpr int FFG_CONV_JOBS = 2; // one-CTA convolutions per launch
+constexpr int FFG_FS_JOBS = 4;   // four-step products (or split pieces) per launch
+struct ConvJobs {
+    ConvJob j[FFG_CONV_JOBS];
+};
+struct FSJobs {
+    FSJob j[FFG_FS_JOBS];
+};
 
-cudaError_t launch_conv_small(const Primes3 &P3, const ConvJob *d_jobs, uint32_t njobs, uint32_t maxL,
+uint32_t crt_ctas(uint64_t nlimbs, uint32_t width); // CTAs (and carry maps) of one CRT
+uint32_t lin_ctas(uint64_t len);                    // CTAs of one linear pass
+
+cudaError_t launch_conv_small(const Primes3 &P3, const ConvJobs &jobs, uint32_t njobs, uint32_t maxL,
                               bool any_distinct, cudaStream_t st, double bytes);
-cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *d_jobs, uint32_t njobs,
+cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t njobs,
                              cudaStream_t st, double limb_bytes);
-cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJob *d_jobs, uint32_t njobs,
+cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJobs &jobs, uint32_t njobs,
                                  cudaStream_t st, double limb_bytes);
-cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob *d_job, uint32_t pairs, cudaStream_t st);
+cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob &job, uint32_t pairs, cudaStream_t st);
 cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st);
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st);
 

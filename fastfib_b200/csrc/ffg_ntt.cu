@@ -23,11 +23,25 @@
 
 namespace ffg {
 
+// Job i of a by-value job list, staged once in shared memory so its fields
+// occupy no registers across the transform (one thread copies it; callers
+// synchronize before use).
+template <typename L, typename T, int N>
+FFG_DEV_INLINE void job_to_smem(const L &list, uint32_t i, T *dst) {
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < N; k++)
+            if (i == (uint32_t)k) *dst = list.j[k];
+    }
+}
+
 // ------------------------------------------------------------ short lengths
 
-__global__ void __launch_bounds__(256) k_conv_small(Primes3 P3, const ConvJob *__restrict__ jobs) {
+__global__ void __launch_bounds__(256, 3) k_conv_small(Primes3 P3, ConvJobs jobs) {
     extern __shared__ uint32_t smem[];
-    const ConvJob J = jobs[blockIdx.x];
+    __shared__ ConvJob J;
+    job_to_smem<ConvJobs, ConvJob, FFG_CONV_JOBS>(jobs, blockIdx.x, &J);
+    __syncthreads();
     const PrimeDev P = P3.pr[blockIdx.y];
     const uint32_t L = J.L_words, p = P.p;
     const uint32_t stride = line_stride(L);
@@ -56,10 +70,12 @@ __global__ void __launch_bounds__(256) k_conv_small(Primes3 P3, const ConvJob *_
 // ------------------------------------------------------------- four-step
 
 // Column tile: columns [c0, c0 + wc) of all R rows, wc lines of length R.
-__global__ void __launch_bounds__(256) k_col_fwd(Primes3 P3, FourStep G, const FSJob *__restrict__ jobs) {
+__global__ void __launch_bounds__(256, 3) k_col_fwd(Primes3 P3, FourStep G, FSJobs jobs) {
     extern __shared__ uint32_t smem[];
     const uint32_t z = blockIdx.z, op = G.square ? 0 : (z & 1), jb = G.square ? z : (z >> 1);
-    const FSJob J = jobs[jb];
+    __shared__ FSJob J;
+    job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, jb, &J);
+    __syncthreads();
     const PrimeDev P = P3.pr[blockIdx.y];
     const uint32_t R = G.R, C = 1u << G.c, wc = G.wc, stride = G.col_stride;
     const uint32_t c0 = blockIdx.x * wc;
@@ -89,9 +105,11 @@ __global__ void __launch_bounds__(256) k_col_fwd(Primes3 P3, FourStep G, const F
 // ROW_FWD: forward transform only (the split's pieces).  ROW_ACC_INV: the
 // split's output piece m, sum over i + j = m of A_i B_j on this row
 // (src/mul_split.c:62-78), then the inverse.
-__global__ void __launch_bounds__(256) k_row_conv(Primes3 P3, FourStep G, const FSJob *__restrict__ jobs) {
+__global__ void __launch_bounds__(256, 3) k_row_conv(Primes3 P3, FourStep G, FSJobs jobs) {
     extern __shared__ uint32_t smem[];
-    const FSJob J = jobs[blockIdx.z];
+    __shared__ FSJob J;
+    job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, blockIdx.z, &J);
+    __syncthreads();
     const PrimeDev P = P3.pr[blockIdx.y];
     const uint32_t C = 1u << G.c, pos = blockIdx.x, p = P.p;
     const uint32_t stride = line_stride(C);
@@ -149,9 +167,11 @@ __global__ void __launch_bounds__(256) k_row_conv(Primes3 P3, FourStep G, const 
     }
 }
 
-__global__ void __launch_bounds__(256) k_col_inv(Primes3 P3, FourStep G, const FSJob *__restrict__ jobs) {
+__global__ void __launch_bounds__(256, 3) k_col_inv(Primes3 P3, FourStep G, FSJobs jobs) {
     extern __shared__ uint32_t smem[];
-    const FSJob J = jobs[blockIdx.z];
+    __shared__ FSJob J;
+    job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, blockIdx.z, &J);
+    __syncthreads();
     const PrimeDev P = P3.pr[blockIdx.y];
     const uint32_t R = G.R, C = 1u << G.c, wc = G.wc, stride = G.col_stride;
     const uint32_t c0 = blockIdx.x * wc;
@@ -193,8 +213,13 @@ static cudaError_t smem_optin() {
     if ((e = cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
     const void *ks[] = {(const void *)k_conv_small, (const void *)k_col_fwd, (const void *)k_row_conv,
                         (const void *)k_col_inv};
-    for (const void *k : ks)
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    for (const void *k : ks) {
+        cudaFuncAttributes fa;
+        if ((e = cudaFuncGetAttributes(&fa, k))) return e; // static shared memory counts against the limit
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      maxsm - (int)fa.sharedSizeBytes)))
+            return e;
+    }
     done = 1;
     return cudaSuccess;
 }
@@ -203,18 +228,18 @@ static size_t small_smem_bytes(uint32_t L, bool square) {
     return (size_t)line_stride(L) * (square ? 1 : 2) * sizeof(uint32_t);
 }
 
-cudaError_t launch_conv_small(const Primes3 &P3, const ConvJob *d_jobs, uint32_t njobs, uint32_t maxL,
+cudaError_t launch_conv_small(const Primes3 &P3, const ConvJobs &jobs, uint32_t njobs, uint32_t maxL,
                               bool any_distinct, cudaStream_t st, double bytes) {
     size_t sm = small_smem_bytes(maxL, !any_distinct);
     cudaError_t e = smem_optin();
     if (e != cudaSuccess) return e;
     prof_begin(PK_CONV_SMALL, st);
-    k_conv_small<<<dim3(njobs, 3, 1), 256, sm, st>>>(P3, d_jobs);
+    k_conv_small<<<dim3(njobs, 3, 1), 256, sm, st>>>(P3, jobs);
     prof_end(PK_CONV_SMALL, st, bytes);
     return cudaGetLastError();
 }
 
-cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *d_jobs, uint32_t njobs,
+cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t njobs,
                              cudaStream_t st, double limb_bytes) {
     size_t sm_col = (size_t)G.col_stride * G.wc * sizeof(uint32_t);
     size_t sm_row = (size_t)line_stride(1u << G.c) * (G.square ? 1 : 2) * sizeof(uint32_t);
@@ -226,15 +251,15 @@ cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJob *
     // (twiddles excluded); the first pass reads limbs instead of residues
     const double res = 3.0 * 4.0 * (double)G.L * njobs;
     prof_begin(PK_COL_FWD, st);
-    k_col_fwd<<<dim3(tiles, 3, njobs * nops), 256, sm_col, st>>>(P3, G, d_jobs);
+    k_col_fwd<<<dim3(tiles, 3, njobs * nops), 256, sm_col, st>>>(P3, G, jobs);
     prof_end(PK_COL_FWD, st, res * nops + limb_bytes);
     if ((e = cudaGetLastError())) return e;
     prof_begin(PK_ROW_CONV, st);
-    k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, d_jobs);
+    k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, jobs);
     prof_end(PK_ROW_CONV, st, res * (nops + 1));
     if ((e = cudaGetLastError())) return e;
     prof_begin(PK_COL_INV, st);
-    k_col_inv<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, d_jobs);
+    k_col_inv<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, jobs);
     prof_end(PK_COL_INV, st, res * 2);
     return cudaGetLastError();
 }
@@ -247,7 +272,7 @@ static cudaError_t cfg_four_step(const FourStep &G, size_t *sm_col, size_t *sm_r
 }
 
 // Forward transforms of njobs pieces (one operand each, G.square = 1).
-cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJob *d_jobs, uint32_t njobs,
+cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJobs &jobs, uint32_t njobs,
                                  cudaStream_t st, double limb_bytes) {
     size_t sm_col, sm_row;
     G.square = 1;
@@ -257,18 +282,20 @@ cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJob *d_j
     const uint32_t tiles = (1u << G.c) / G.wc;
     const double res = 3.0 * 4.0 * (double)G.L * njobs;
     prof_begin(PK_COL_FWD, st);
-    k_col_fwd<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, d_jobs);
+    k_col_fwd<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, jobs);
     prof_end(PK_COL_FWD, st, res + limb_bytes);
     if ((e = cudaGetLastError())) return e;
     prof_begin(PK_ROW_CONV, st);
-    k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, d_jobs);
+    k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, jobs);
     prof_end(PK_ROW_CONV, st, res * 2);
     return cudaGetLastError();
 }
 
 // One output piece: pairwise sum + inverse row pass, then the inverse column
 // pass adding into the whole product's residues.  pairs: products summed.
-cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob *d_job, uint32_t pairs, cudaStream_t st) {
+cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob &job, uint32_t pairs, cudaStream_t st) {
+    FSJobs one{};
+    one.j[0] = job;
     size_t sm_col, sm_row;
     G.square = 1;
     G.mode = ROW_ACC_INV;
@@ -277,11 +304,11 @@ cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob *d_job
     const uint32_t tiles = (1u << G.c) / G.wc;
     const double res = 3.0 * 4.0 * (double)G.L;
     prof_begin(PK_ROW_CONV, st);
-    k_row_conv<<<dim3(G.R, 3, 1), 256, sm_row, st>>>(P3, G, d_job);
+    k_row_conv<<<dim3(G.R, 3, 1), 256, sm_row, st>>>(P3, G, one);
     prof_end(PK_ROW_CONV, st, res * (2.0 * pairs + 1.0));
     if ((e = cudaGetLastError())) return e;
     prof_begin(PK_COL_INV, st);
-    k_col_inv<<<dim3(tiles, 3, 1), 256, sm_col, st>>>(P3, G, d_job);
+    k_col_inv<<<dim3(tiles, 3, 1), 256, sm_col, st>>>(P3, G, one);
     prof_end(PK_COL_INV, st, res * 3.0);
     return cudaGetLastError();
 }

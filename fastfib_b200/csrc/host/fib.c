@@ -69,10 +69,7 @@ Big fibonacci(uint64_t n) {
         if (rc) ff_gpu_failed("fibonacci chain", ffg_last_error());
         big_free(&fkm1);
         big_free(&fk);
-        Big r = {xmalloc(nd * sizeof(uint64_t)), nd};
-        for (size_t j = 0; j < nd; j++) r.d[j] = d[j];
-        ffg_free(d);
-        return r;
+        return (Big){d, nd}; /* malloc'ed by the layer: big_free releases it */
     }
     /* short n: the last bit here as well */
     Big result;
