@@ -102,11 +102,20 @@ static cudaEvent_t ev_get() {
     return e;
 }
 
+static bool g_capturing = false, g_capture_starved = false;
+
+// Inside a stream capture an event becomes a timing node of the graph only
+// when recorded as external.
+static void ev_record(cudaEvent_t e, cudaStream_t st) {
+    if (g_capturing) cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+    else cudaEventRecord(e, st);
+}
+
 void prof_begin(int kind, cudaStream_t st) {
     g_launches++;
     if (!g_prof_on || !((g_prof_mask >> kind) & 1)) return;
     ProfPair pp{kind, ev_get(), nullptr, 0};
-    cudaEventRecord(pp.a, st);
+    ev_record(pp.a, st);
     g_prof_open.push_back(pp);
 }
 
@@ -116,7 +125,7 @@ void prof_end(int kind, cudaStream_t st, double bytes) {
     ProfPair &pp = g_prof_open.back();
     pp.b = ev_get();
     pp.bytes = bytes;
-    cudaEventRecord(pp.b, st);
+    ev_record(pp.b, st);
 }
 
 // Folds finished brackets into the totals (synchronizes on their events).
@@ -245,6 +254,10 @@ static void arena_reset() {
     for (auto &b : g.blocks) b.used = 0;
 }
 
+// g_capturing is set while a stream capture is open: the arena must not grow
+// then (no cudaMalloc may be issued); a request that would need a new block
+// fails and the capture is abandoned.
+
 static void *arena_alloc(size_t bytes) {
     bytes = (bytes + 255) & ~(size_t)255;
     for (auto &b : g.blocks)
@@ -253,6 +266,10 @@ static void *arena_alloc(size_t bytes) {
             b.used += bytes;
             return p;
         }
+    if (g_capturing) {
+        g_capture_starved = true;
+        return nullptr;
+    }
     size_t last = g.blocks.empty() ? 0 : g.blocks.back().cap;
     size_t cap = std::max(bytes, std::max((size_t)64 << 20, 2 * last));
     char *p = nullptr;
@@ -602,21 +619,15 @@ static int lin(const uint64_t *s1, uint64_t n1, const uint64_t *s2, uint64_t n2,
     return FFG_OK;
 }
 
-static int fib_chain(uint64_t n, int i0, const uint64_t *hkm1, size_t hnkm1, const uint64_t *hk, size_t hnk,
-                     uint64_t **out, size_t *nout) {
-    cudaStream_t st = g.stream;
+// The device part of the chain, from the pair (F(k-1), F(k)) in fkm1 / fk
+// (bit lengths bkm1 / bk) to F(n) in *res (*nres limbs, leading zeros
+// allowed): kernel launches and arena allocations only, in the same order on
+// every call, so a CUDA graph can capture it.
+static int chain_body(uint64_t n, int i0, uint64_t *fk, uint64_t *fkm1, uint64_t bk, uint64_t bkm1,
+                      uint64_t **res_out, uint64_t *nres_out, cudaStream_t st) {
     uint64_t k = n >> i0;
     int kodd = (int)(k & 1);
-    uint64_t nk = hnk ? hnk : 1, nkm1 = hnkm1 ? hnkm1 : 1;
-    uint64_t cap0 = std::max(nk, nkm1);
-    ALLOC(fk, uint64_t, cap0);
-    ALLOC(fkm1, uint64_t, cap0);
-    CK(cudaMemsetAsync(fk, 0, cap0 * 8, st));
-    CK(cudaMemsetAsync(fkm1, 0, cap0 * 8, st));
-    CK(cudaMemcpyAsync(fk, hk, hnk * 8, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(fkm1, hkm1, hnkm1 * 8, cudaMemcpyHostToDevice, st));
-    uint64_t bk = bits_of(hk, hnk), bkm1 = bits_of(hkm1, hnkm1);
-    CK(cudaEventRecord(g.ev0, st));
+    uint64_t nk, nkm1;
     for (int i = i0 - 1; i >= 1; i--) {
         const int bit = (int)((n >> i) & 1);
         if (bkm1 == 0) bkm1 = 1;
@@ -686,7 +697,122 @@ static int fib_chain(uint64_t n, int i0, const uint64_t *hkm1, size_t hnkm1, con
         rc = mul_one(p, false, st);
     }
     if (rc) return rc;
-    CK(cudaEventRecord(g.ev1, st));
+    *res_out = res;
+    *nres_out = nres;
+    return FFG_OK;
+}
+
+// A captured chain for one n (and one starting pair size), replayed by later
+// calls: the pair is copied into the same device buffers and the graph runs.
+struct ChainGraph {
+    uint64_t n;
+    int i0;
+    uint64_t max_L;   // plans depend on the transform cap
+    uint64_t hnk, hnkm1;
+    uint32_t prof_mask;
+    uint64_t *fk, *fkm1, *res;
+    uint64_t nres;
+    int eager_runs;
+    cudaGraphExec_t exec;
+    uint64_t launches;
+    std::vector<ProfPair> prof;
+};
+static std::vector<ChainGraph> g_chains;
+
+static bool graphs_enabled() {
+    const char *e = getenv("FFG_NO_GRAPH");
+    return !(e && *e && *e != '0');
+}
+
+static int fib_chain(uint64_t n, int i0, const uint64_t *hkm1, size_t hnkm1, const uint64_t *hk, size_t hnk,
+                     uint64_t **out, size_t *nout) {
+    cudaStream_t st = g.stream;
+    const uint64_t nk = hnk ? hnk : 1, nkm1 = hnkm1 ? hnkm1 : 1;
+    const uint64_t cap0 = std::max(nk, nkm1);
+    ALLOC(fk, uint64_t, cap0);
+    ALLOC(fkm1, uint64_t, cap0);
+    CK(cudaMemsetAsync(fk, 0, cap0 * 8, st));
+    CK(cudaMemsetAsync(fkm1, 0, cap0 * 8, st));
+    CK(cudaMemcpyAsync(fk, hk, hnk * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(fkm1, hkm1, hnkm1 * 8, cudaMemcpyHostToDevice, st));
+    const uint64_t bk = bits_of(hk, hnk), bkm1 = bits_of(hkm1, hnkm1);
+    const uint32_t mask = g_prof_on ? g_prof_mask : 0;
+
+    ChainGraph *cg = nullptr;
+    for (auto &c : g_chains)
+        if (c.n == n && c.i0 == i0 && c.max_L == g.max_L && c.hnk == hnk && c.hnkm1 == hnkm1 &&
+            c.prof_mask == mask)
+            cg = &c;
+    uint64_t *res = nullptr, nres = 0;
+    if (cg && cg->exec && cg->fk == fk && cg->fkm1 == fkm1) {
+        CK(cudaEventRecord(g.ev0, st));
+        CK(cudaGraphLaunch(cg->exec, st));
+        CK(cudaEventRecord(g.ev1, st));
+        g_launches += cg->launches;
+        res = cg->res;
+        nres = cg->nres;
+    } else {
+        bool capture = graphs_enabled() && cg && cg->eager_runs >= 1 && cg->fk == fk && cg->fkm1 == fkm1;
+        const uint64_t launches0 = g_launches;
+        const size_t prof0 = g_prof_open.size();
+        const auto marks = g.blocks; // arena state after the pair, to rerun eagerly from
+        CK(cudaEventRecord(g.ev0, st));
+        int rc = FFG_OK;
+        if (capture) {
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            g_capturing = true;
+            g_capture_starved = false;
+            rc = chain_body(n, i0, fk, fkm1, bk, bkm1, &res, &nres, st);
+            g_capturing = false;
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamEndCapture(st, &graph);
+            cudaGraphExec_t exec = nullptr;
+            if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (rc || e != cudaSuccess) {
+                // abandoned (e.g. the arena would have had to grow): run eagerly
+                cudaGetLastError();
+                if (exec) cudaGraphExecDestroy(exec);
+                for (size_t b = 0; b < g.blocks.size(); b++) g.blocks[b].used = b < marks.size() ? marks[b].used : 0;
+                for (size_t q = prof0; q < g_prof_open.size(); q++) {
+                    g_ev_pool.push_back(g_prof_open[q].a);
+                    if (g_prof_open[q].b) g_ev_pool.push_back(g_prof_open[q].b);
+                }
+                g_prof_open.resize(prof0);
+                g_launches = launches0;
+                capture = false;
+            }
+            if (!capture) {
+                rc = chain_body(n, i0, fk, fkm1, bk, bkm1, &res, &nres, st);
+                if (rc) return rc;
+                cg->eager_runs++;
+                CK(cudaEventRecord(g.ev1, st));
+                goto copy_back;
+            }
+            cg->exec = exec;
+            cg->res = res;
+            cg->nres = nres;
+            cg->launches = g_launches - launches0;
+            // the captured event brackets belong to the graph from now on
+            cg->prof.assign(g_prof_open.begin() + prof0, g_prof_open.end());
+            g_prof_open.resize(prof0);
+            CK(cudaGraphLaunch(exec, st));
+        } else {
+            rc = chain_body(n, i0, fk, fkm1, bk, bkm1, &res, &nres, st);
+            if (rc) return rc;
+            if (!cg) {
+                if (g_chains.size() >= 8) {
+                    if (g_chains.front().exec) cudaGraphExecDestroy(g_chains.front().exec);
+                    g_chains.erase(g_chains.begin());
+                }
+                g_chains.push_back(ChainGraph{n, i0, g.max_L, hnk, hnkm1, mask, fk, fkm1, nullptr, 0, 0, nullptr, 0, {}});
+                cg = &g_chains.back();
+            }
+            cg->eager_runs++;
+        }
+        CK(cudaEventRecord(g.ev1, st));
+    }
+copy_back:
     uint64_t *h = (uint64_t *)malloc(nres * 8);
     if (!h) return fail(FFG_E_NOMEM, "host: %zu bytes", (size_t)nres * 8);
     CK(cudaMemcpyAsync(h, res, nres * 8, cudaMemcpyDeviceToHost, st));
@@ -694,6 +820,16 @@ static int fib_chain(uint64_t n, int i0, const uint64_t *hkm1, size_t hnkm1, con
     if (e) {
         free(h);
         return fail(FFG_E_CUDA, "fib chain: %s", cudaGetErrorString(e));
+    }
+    if (cg && cg->exec) { // a replay (or the capture's first run): its brackets
+        for (auto &pp : cg->prof) {
+            float ms = 0;
+            if (pp.b && cudaEventElapsedTime(&ms, pp.a, pp.b) == cudaSuccess) {
+                g_prof_ms[pp.kind] += ms;
+                g_prof_bytes[pp.kind] += pp.bytes;
+                g_prof_n[pp.kind]++;
+            }
+        }
     }
     float ms = 0;
     cudaEventElapsedTime(&ms, g.ev0, g.ev1);

@@ -53,8 +53,13 @@ def test_fingerprints(ff, n):
     assert fingerprint(ff.fibonacci(n), primes) == [int(v) for v in gold["fingerprints"][str(n)]]
 
 
-def test_repeatable(ff):
-    """The chain reuses its device arena: repeated calls give identical limbs."""
-    a = ff.fibonacci(10**7)
-    b = ff.fibonacci(10**7)
-    assert np.array_equal(a, b)
+def test_repeatable(ff, oracle):
+    """The chain runs eagerly once, is captured into a CUDA graph on the second
+    call and replayed after that: every call gives the oracle's limbs."""
+    want = oracle.fibonacci(10**7 + 19)
+    for _ in range(4):
+        assert np.array_equal(ff.fibonacci(10**7 + 19), want)
+    other = oracle.fibonacci(3 * 10**6)
+    for _ in range(3):  # a second cached chain next to the first
+        assert np.array_equal(ff.fibonacci(3 * 10**6), other)
+        assert np.array_equal(ff.fibonacci(10**7 + 19), want)
