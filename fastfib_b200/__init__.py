@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -79,6 +80,7 @@ def lib() -> ctypes.CDLL:
     L.ffg_launch_count.restype = ctypes.c_uint64
     L.ffg_last_error.restype = ctypes.c_char_p
     L.ffg_free.argtypes = [ctypes.c_void_p]
+    L.ffg_release.argtypes = [ctypes.c_void_p]
     for name in ("big_mul", "big_mul_ntt", "big_mul_toom3"):
         getattr(L, name).restype = Big
         getattr(L, name).argtypes = [ctypes.POINTER(Big), ctypes.POINTER(Big)]
@@ -114,9 +116,15 @@ def _view(a: np.ndarray) -> Big:
     return Big(a.ctypes.data_as(_u64p), n)
 
 
+def _release(big: Big) -> None:
+    lib().big_free(ctypes.byref(big))
+
+
 def _take(b: Big) -> np.ndarray:
-    out = np.ctypeslib.as_array(b.d, shape=(b.n,)).copy()
-    lib().big_free(ctypes.byref(b))
+    """The Big's limbs as a numpy array that owns them (no copy); the limbs
+    are released with big_free when the array is collected."""
+    out = np.ctypeslib.as_array(b.d, shape=(b.n,))
+    weakref.finalize(out, _release, Big(b.d, b.n))
     return out
 
 

@@ -719,6 +719,48 @@ struct ChainGraph {
 };
 static std::vector<ChainGraph> g_chains;
 
+// Results come back to the host in pinned buffers (a DMA straight into the
+// caller's memory, no staging copy).  They are pooled: ffg_free / ffg_release
+// return one to the pool, and the next result of a fitting size reuses it.
+static std::vector<std::pair<void *, size_t>> g_pinned_out, g_pinned_pool;
+static volatile size_t g_pinned_outstanding = 0;
+
+static void *pinned_get(size_t bytes) {
+    size_t best = (size_t)-1;
+    for (size_t i = 0; i < g_pinned_pool.size(); i++)
+        if (g_pinned_pool[i].second >= bytes &&
+            (best == (size_t)-1 || g_pinned_pool[i].second < g_pinned_pool[best].second))
+            best = i;
+    std::pair<void *, size_t> b;
+    if (best != (size_t)-1) {
+        b = g_pinned_pool[best];
+        g_pinned_pool.erase(g_pinned_pool.begin() + best);
+    } else {
+        size_t cap = std::max(bytes, (size_t)1 << 20);
+        void *p = nullptr;
+        if (cudaMallocHost(&p, cap) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        b = {p, cap};
+    }
+    g_pinned_out.push_back(b);
+    g_pinned_outstanding = g_pinned_out.size();
+    return b.first;
+}
+
+// Returns 1 if p is a pooled result buffer (now back in the pool), else 0.
+static int pinned_release(void *p) {
+    for (size_t i = 0; i < g_pinned_out.size(); i++)
+        if (g_pinned_out[i].first == p) {
+            g_pinned_pool.push_back(g_pinned_out[i]);
+            g_pinned_out.erase(g_pinned_out.begin() + i);
+            g_pinned_outstanding = g_pinned_out.size();
+            return 1;
+        }
+    return 0;
+}
+
 static bool graphs_enabled() {
     const char *e = getenv("FFG_NO_GRAPH");
     return !(e && *e && *e != '0');
@@ -813,12 +855,12 @@ static int fib_chain(uint64_t n, int i0, const uint64_t *hkm1, size_t hnkm1, con
         CK(cudaEventRecord(g.ev1, st));
     }
 copy_back:
-    uint64_t *h = (uint64_t *)malloc(nres * 8);
-    if (!h) return fail(FFG_E_NOMEM, "host: %zu bytes", (size_t)nres * 8);
+    uint64_t *h = (uint64_t *)pinned_get(nres * 8);
+    if (!h) return fail(FFG_E_NOMEM, "pinned host buffer: %zu bytes", (size_t)nres * 8);
     CK(cudaMemcpyAsync(h, res, nres * 8, cudaMemcpyDeviceToHost, st));
     cudaError_t e = cudaStreamSynchronize(st);
     if (e) {
-        free(h);
+        pinned_release(h);
         return fail(FFG_E_CUDA, "fib chain: %s", cudaGetErrorString(e));
     }
     if (cg && cg->exec) { // a replay (or the capture's first run): its brackets
@@ -978,7 +1020,15 @@ extern "C" int ffg_profile_read(int kind, uint64_t *launches, double *ms, double
 
 extern "C" uint64_t ffg_launch_count(void) { return g_launches; }
 extern "C" const char *ffg_last_error(void) { return g.err.c_str(); }
-extern "C" void ffg_free(void *p) { free(p); }
+extern "C" int ffg_release(void *p) {
+    if (!p || !g_pinned_outstanding) return 0;
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    return pinned_release(p);
+}
+
+extern "C" void ffg_free(void *p) {
+    if (!ffg_release(p)) free(p);
+}
 
 extern "C" void ffg_shutdown(void) {
     std::lock_guard<std::recursive_mutex> lk(g_mu);
@@ -988,6 +1038,8 @@ extern "C" void ffg_shutdown(void) {
     g.blocks.clear();
     cudaFree(g.tables);
     g.tables = nullptr;
+    for (auto &b : g_pinned_pool) cudaFreeHost(b.first);
+    g_pinned_pool.clear();
     cudaEventDestroy(g.ev0);
     cudaEventDestroy(g.ev1);
     cudaStreamDestroy(g.stream);

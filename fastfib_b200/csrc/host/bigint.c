@@ -10,6 +10,7 @@
 #include <time.h>
 
 #include "fastfib.h"
+#include "ffg.h"
 #include "host_internal.h"
 
 /* The reference ends the program with a message when memory runs out
@@ -36,7 +37,11 @@ void *xcalloc(size_t n, size_t size) {
     return p;
 }
 
-void xfree(void *p) { free(p); }
+/* Results of the device chain live in the layer's pinned buffers; everything
+   else is the C heap. */
+void xfree(void *p) {
+    if (!ffg_release(p)) free(p);
+}
 
 /* The shared zero of empty views: never written, never freed (src/common.h:38-40). */
 uint64_t g_zero_limb = 0;

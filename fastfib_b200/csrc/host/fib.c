@@ -69,7 +69,7 @@ Big fibonacci(uint64_t n) {
         if (rc) ff_gpu_failed("fibonacci chain", ffg_last_error());
         big_free(&fkm1);
         big_free(&fk);
-        return (Big){d, nd}; /* malloc'ed by the layer: big_free releases it */
+        return (Big){d, nd}; /* the layer's pinned buffer: big_free returns it */
     }
     /* short n: the last bit here as well */
     Big result;

@@ -91,7 +91,7 @@ int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t na, uint64_t
 
 /* fibonacci (src/fib.c:211) from bit i0 down: continues fast doubling from
    the pair (F(k-1), F(k)), k = n >> i0, on the device and returns F(n) as a
-   malloc'ed limb array (free with ffg_free).  i0 >= 1. */
+   limb array in pinned host memory (free with ffg_free).  i0 >= 1. */
 int ffg_fib_chain(uint64_t n, int i0, const uint64_t *fkm1, size_t nkm1, const uint64_t *fk, size_t nk,
                   uint64_t **out, size_t *nout);
 
@@ -117,7 +117,12 @@ int ffg_profile_read(int kind, uint64_t *launches, double *ms, double *bytes);
 uint64_t ffg_launch_count(void);
 
 const char *ffg_last_error(void);
+/* Frees an array this layer returned (ffg_fib_chain's results live in a
+   pool of pinned host buffers; anything else is plain malloc memory). */
 void ffg_free(void *p);
+/* Returns 1 and takes p back into the pool if it is one of this layer's
+   pinned result buffers, else 0 (p untouched). */
+int ffg_release(void *p);
 /* Releases device memory, streams and tables. */
 void ffg_shutdown(void);
 
