@@ -44,6 +44,17 @@ class Plan(ctypes.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
+class Job(ctypes.Structure):
+    """ffg_job (include/ffg.h)."""
+    _fields_ = [("a", _u64p), ("b", _u64p), ("na", ctypes.c_uint64), ("nb", ctypes.c_uint64),
+                ("bits_a", ctypes.c_uint64), ("bits_b", ctypes.c_uint64), ("out", _u64p),
+                ("nout", ctypes.c_uint64), ("square", ctypes.c_int32), ("method", ctypes.c_int32)]
+
+
+# methods of a batched product (FFG_M_*)
+METHODS = {"plain": -1, "school": 0, "ntt": 1, "ntt_pow2": 2, "ntt_r3": 3}
+
+
 class FfgError(RuntimeError):
     pass
 
@@ -80,6 +91,8 @@ def lib() -> ctypes.CDLL:
     L.ffg_launch_count.restype = ctypes.c_uint64
     L.ffg_last_error.restype = ctypes.c_char_p
     L.ffg_free.argtypes = [ctypes.c_void_p]
+    L.ffg_mul_batch_host.argtypes = [ctypes.POINTER(Job), ctypes.c_size_t]
+    L.ffg_mul_batch_device.argtypes = [ctypes.POINTER(Job), ctypes.c_size_t, ctypes.c_void_p]
     L.ffg_release.argtypes = [ctypes.c_void_p]
     for name in ("big_mul", "big_mul_ntt", "big_mul_toom3"):
         getattr(L, name).restype = Big
@@ -218,6 +231,45 @@ def mul(a, b=None) -> np.ndarray:
     return out[: n.value].copy()
 
 
+def mul_batch(pairs, method="ntt") -> list:
+    """ffg_mul_batch_host: many independent products in one call.  pairs holds
+    (a, b) with b None for a square; method names one of METHODS, or is a list
+    with one name per product."""
+    arrs, jobs = [], (Job * max(1, len(pairs)))()
+    outs = []
+    for i, (a, b) in enumerate(pairs):
+        a = _arr(a)
+        sq = b is None
+        b = a if sq else _arr(b)
+        out = np.zeros(a.size + b.size, dtype=np.uint64)
+        arrs += [a, b]
+        outs.append(out)
+        m = method[i] if isinstance(method, (list, tuple)) else method
+        j = jobs[i]
+        j.a, j.b = a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p)
+        j.na, j.nb = a.size, b.size
+        j.out = out.ctypes.data_as(_u64p)
+        j.square, j.method = int(sq), METHODS[m]
+    _check(lib().ffg_mul_batch_host(jobs, len(pairs)))
+    return [outs[i][: jobs[i].nout].copy() for i in range(len(pairs))]
+
+
+def mul_batch_device(jobs, stream: int = 0) -> None:
+    """ffg_mul_batch_device on a list of dicts with device pointers:
+    a, b, na, nb, bits_a, bits_b, out (na + nb + 1 limbs), square, method."""
+    arr = (Job * max(1, len(jobs)))()
+    for i, d in enumerate(jobs):
+        j = arr[i]
+        j.a = ctypes.cast(d["a"], _u64p)
+        j.b = ctypes.cast(d.get("b") or d["a"], _u64p)
+        j.na, j.nb = d["na"], d.get("nb", d["na"])
+        j.bits_a, j.bits_b = d["bits_a"], d.get("bits_b", d["bits_a"])
+        j.out = ctypes.cast(d["out"], _u64p)
+        j.square = int(d.get("square", False))
+        j.method = METHODS[d.get("method", "ntt")]
+    _check(lib().ffg_mul_batch_device(arr, len(jobs), stream or None))
+
+
 def mul_device(out_ptr: int, a_ptr: int, na: int, bits_a: int, b_ptr: int, nb: int, bits_b: int,
                square: bool = False, stream: int = 0) -> None:
     """ffg_mul_device on device pointers (e.g. torch tensors' data_ptr())."""
@@ -240,7 +292,7 @@ def last_chain_ms() -> float:
     return lib().ffg_last_chain_ms()
 
 
-KERNEL_FAMILIES = ("conv_small", "col_fwd", "row_conv", "col_inv", "crt", "carry", "lin")
+KERNEL_FAMILIES = ("conv_small", "col_fwd", "row_conv", "col_inv", "crt", "carry", "lin", "school")
 
 
 def profile(families=None) -> None:

@@ -34,7 +34,24 @@ constexpr uint32_t CRT_NL_PER_W = 32;   // limbs per CTA = 32 * width
 
 FFG_DEV_INLINE int64_t floor_div(int64_t a, int64_t b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
-__global__ void __launch_bounds__(CRT_THREADS) k_crt(GarnerConst K, CrtJob J) {
+FFG_DEV_INLINE uint32_t crt_ctas_dev(uint64_t nlimbs, uint32_t width) {
+    const uint64_t NL = (uint64_t)CRT_NL_PER_W * width;
+    return (uint32_t)((nlimbs + NL - 1) / NL);
+}
+
+FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t cta);
+
+__global__ void __launch_bounds__(CRT_THREADS) k_crt(GarnerConst K, CrtJob J) { crt_block(K, J, blockIdx.x); }
+
+// A batch of CRTs: product blockIdx.y, its CTA blockIdx.x (CTAs past the
+// product's own count return at once, all threads together).
+__global__ void __launch_bounds__(CRT_THREADS) k_crt_batch(GarnerConst K, const CrtJob *__restrict__ jobs) {
+    const CrtJob J = jobs[blockIdx.y];
+    if (blockIdx.x >= crt_ctas_dev(J.nlimbs, J.width)) return;
+    crt_block(K, J, blockIdx.x);
+}
+
+FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t cta) {
     extern __shared__ __align__(16) unsigned char sm[];
     uint64_t *Xlo = (uint64_t *)sm;                              // CRT_COEF + halo
     uint64_t *lo = Xlo + CRT_COEF + CRT_HALO_MAX;                // NL limbs
@@ -45,7 +62,7 @@ __global__ void __launch_bounds__(CRT_THREADS) k_crt(GarnerConst K, CrtJob J) {
 
     const uint32_t b = J.width, NL = CRT_NL_PER_W * b;
     const int32_t halo = (int32_t)(((156 + b - 1) / b + 1 + 3) & ~3u);
-    const int64_t ibase = (int64_t)blockIdx.x * CRT_COEF;
+    const int64_t ibase = (int64_t)cta * CRT_COEF;
     const uint32_t p1 = K.p[0], p2 = K.p[1], p3 = K.p[2];
 
     // residues in 16-byte vectors of 4 coefficients, every load of the thread
@@ -92,7 +109,7 @@ __global__ void __launch_bounds__(CRT_THREADS) k_crt(GarnerConst K, CrtJob J) {
     __syncthreads();
 
     // column sums; j = -1 (the limb below the CTA) only for its high part
-    const uint64_t j0 = (uint64_t)blockIdx.x * NL;
+    const uint64_t j0 = (uint64_t)cta * NL;
     const bool neg_add = J.add < 0;
     for (int32_t j = (int32_t)threadIdx.x - 1; j < (int32_t)NL; j += blockDim.x) {
         const int64_t ilo = floor_div(64 * (int64_t)j - 92 + b - 1, b), ihi = floor_div(64 * (int64_t)j + 63, b);
@@ -119,17 +136,33 @@ __global__ void __launch_bounds__(CRT_THREADS) k_crt(GarnerConst K, CrtJob J) {
         }
     }
     __syncthreads();
-    const uint32_t map = cta_resolve(lo, hi, blockIdx.x ? hiprev_s : 0, NL, gG, gP, gin);
+    const uint32_t map = cta_resolve(lo, hi, cta ? hiprev_s : 0, NL, gG, gP, gin);
     for (uint32_t j = threadIdx.x; j < NL && j0 + j < J.nlimbs; j += blockDim.x) J.out[j0 + j] = lo[j];
-    if (threadIdx.x == 0) J.maps[blockIdx.x] = map;
+    if (threadIdx.x == 0) J.maps[cta] = map;
 }
 
 // Carries between CTAs: one warp per 32 CTAs composes the maps of every CTA
 // before them (from carry 0 into the first), then each lane whose CTA
 // receives a carry adds it into that CTA's lowest limbs.
+FFG_DEV_INLINE void settle_warp(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *__restrict__ maps,
+                                uint32_t ncta, uint32_t group);
+
 __global__ void __launch_bounds__(32) k_settle(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs,
                                                const uint32_t *__restrict__ maps, uint32_t ncta) {
-    const uint32_t lane = threadIdx.x, first = blockIdx.x * 32;
+    settle_warp(out, nlimbs, cta_limbs, maps, ncta, blockIdx.x);
+}
+
+// Settles a batch of CRTs (blockIdx.y the product).
+__global__ void __launch_bounds__(32) k_settle_crt_batch(const CrtJob *__restrict__ jobs) {
+    const CrtJob J = jobs[blockIdx.y];
+    const uint32_t ncta = crt_ctas_dev(J.nlimbs, J.width);
+    if (ncta <= 1 || blockIdx.x * 32 >= ncta) return;
+    settle_warp(J.out, J.nlimbs, CRT_NL_PER_W * J.width, J.maps, ncta, blockIdx.x);
+}
+
+FFG_DEV_INLINE void settle_warp(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *__restrict__ maps,
+                                uint32_t ncta, uint32_t group) {
+    const uint32_t lane = threadIdx.x, first = group * 32;
     uint32_t carry = 0;
     for (uint32_t base = 0; base < first; base += 32) {
         const uint32_t m = maps[base + lane]; // base + 32 <= first <= ncta
@@ -183,6 +216,114 @@ cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st) {
     e = launch_settle(J.out, J.nlimbs, CRT_NL_PER_W * J.width, J.maps, ncta, st);
     prof_end(PK_CARRY, st, 4.0 * ncta);
     return e;
+}
+
+cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
+                             double bytes) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e =
+            cudaFuncSetAttribute(k_crt_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)crt_smem());
+        if (e) return e;
+        configured = true;
+    }
+    if (!count) return cudaSuccess;
+    prof_begin(PK_CRT, st);
+    k_crt_batch<<<dim3(max_ctas, count), CRT_THREADS, crt_smem(), st>>>(garner_const(), d_jobs);
+    prof_end(PK_CRT, st, bytes);
+    cudaError_t e = cudaGetLastError();
+    if (e || max_ctas <= 1) return e;
+    prof_begin(PK_CARRY, st);
+    k_settle_crt_batch<<<dim3((max_ctas + 31) / 32, count), 32, 0, st>>>(d_jobs);
+    prof_end(PK_CARRY, st, 4.0 * max_ctas * count);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------- schoolbook
+
+// k_school: a batch of schoolbook products (blockIdx.y the product), 256
+// threads per CTA and SCHOOL_NL output limbs (columns) per CTA.  Column j
+// sums a_i b_(j-i) over the shorter operand into 192 bits (t0, t1, t2); then
+// v_j = t0_j + t1_(j-1) + t2_(j-2) < 3 2^64 leaves single-bit ripples for
+// cta_resolve, and carries between CTAs go through k_settle_school.
+constexpr uint32_t SCHOOL_NL = 1024;
+constexpr uint32_t SCHOOL_THREADS = 256;
+
+__host__ __device__ uint32_t school_ctas(uint64_t nlimbs) { return (uint32_t)((nlimbs + SCHOOL_NL - 1) / SCHOOL_NL); }
+
+FFG_DEV_INLINE void school_col(const SchoolJob &J, int64_t j, uint64_t &t0, uint64_t &t1, uint64_t &t2) {
+    t0 = t1 = t2 = 0;
+    if (j < 0 || (uint64_t)j >= J.na + J.nb - 1) return;
+    // iterate over the shorter operand
+    const bool a_short = J.na <= J.nb;
+    const uint64_t *S = a_short ? J.a : J.b, *Lg = a_short ? J.b : J.a;
+    const int64_t ns = (int64_t)(a_short ? J.na : J.nb), nl = (int64_t)(a_short ? J.nb : J.na);
+    const int64_t i0 = j - nl + 1 > 0 ? j - nl + 1 : 0, i1 = j < ns - 1 ? j : ns - 1;
+    for (int64_t i = i0; i <= i1; i++) {
+        const u128 pr = (u128)__ldg(&S[i]) * __ldg(&Lg[j - i]);
+        const uint64_t lo = (uint64_t)pr, hi = (uint64_t)(pr >> 64);
+        t0 += lo;
+        const uint64_t c0 = t0 < lo;
+        const uint64_t h = hi + c0; // hi < 2^64 - 1, so no wrap
+        t1 += h;
+        t2 += t1 < h;
+    }
+}
+
+__global__ void __launch_bounds__(SCHOOL_THREADS) k_school(const SchoolJob *__restrict__ jobs) {
+    constexpr uint32_t NC = SCHOOL_NL + 3; // columns j0 - 3 .. j0 + NL - 1
+    __shared__ uint64_t t0s[NC], t1s[NC];
+    __shared__ uint32_t t2s[NC];
+    __shared__ uint64_t lo[SCHOOL_NL];
+    __shared__ uint32_t hi[SCHOOL_NL];
+    __shared__ uint32_t gG[SCHOOL_NL / 32], gP[SCHOOL_NL / 32], gin[SCHOOL_NL / 32];
+    __shared__ uint32_t hiprev_s;
+    const SchoolJob J = jobs[blockIdx.y];
+    if (blockIdx.x >= school_ctas(J.nlimbs)) return;
+    const int64_t j0 = (int64_t)blockIdx.x * SCHOOL_NL;
+    for (uint32_t c = threadIdx.x; c < NC; c += blockDim.x) {
+        uint64_t a, b, d;
+        school_col(J, j0 - 3 + (int64_t)c, a, b, d);
+        t0s[c] = a;
+        t1s[c] = b;
+        t2s[c] = (uint32_t)d;
+    }
+    __syncthreads();
+    // v_j = t0_j + t1_(j-1) + t2_(j-2), for j = j0 - 1 .. j0 + NL - 1
+    for (int32_t jl = (int32_t)threadIdx.x - 1; jl < (int32_t)SCHOOL_NL; jl += blockDim.x) {
+        const uint32_t c = (uint32_t)(jl + 3);
+        const u128 v = (u128)t0s[c] + t1s[c - 1] + t2s[c - 2];
+        if (jl < 0) hiprev_s = (uint32_t)(v >> 64);
+        else {
+            lo[jl] = (uint64_t)v;
+            hi[jl] = (uint32_t)(v >> 64);
+        }
+    }
+    __syncthreads();
+    const uint32_t map = cta_resolve(lo, hi, blockIdx.x ? hiprev_s : 0, SCHOOL_NL, gG, gP, gin);
+    for (uint32_t j = threadIdx.x; j < SCHOOL_NL && (uint64_t)j0 + j < J.nlimbs; j += blockDim.x) J.out[j0 + j] = lo[j];
+    if (threadIdx.x == 0) J.maps[blockIdx.x] = map;
+}
+
+__global__ void __launch_bounds__(32) k_settle_school_batch(const SchoolJob *__restrict__ jobs) {
+    const SchoolJob J = jobs[blockIdx.y];
+    const uint32_t ncta = school_ctas(J.nlimbs);
+    if (ncta <= 1 || blockIdx.x * 32 >= ncta) return;
+    settle_warp(J.out, J.nlimbs, SCHOOL_NL, J.maps, ncta, blockIdx.x);
+}
+
+cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
+                                double bytes) {
+    if (!count) return cudaSuccess;
+    prof_begin(PK_SCHOOL, st);
+    k_school<<<dim3(max_ctas, count), SCHOOL_THREADS, 0, st>>>(d_jobs);
+    prof_end(PK_SCHOOL, st, bytes);
+    cudaError_t e = cudaGetLastError();
+    if (e || max_ctas <= 1) return e;
+    prof_begin(PK_CARRY, st);
+    k_settle_school_batch<<<dim3((max_ctas + 31) / 32, count), 32, 0, st>>>(d_jobs);
+    prof_end(PK_CARRY, st, 4.0 * max_ctas * count);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------ linear passes

@@ -9,6 +9,8 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "ffg.h"
@@ -884,6 +886,202 @@ copy_back:
     return FFG_OK;
 }
 
+// ------------------------------------------------------------ batches
+
+// A product of a batch with its method resolved: schoolbook, or an NTT plan.
+struct BJob {
+    const uint64_t *a, *b;
+    uint64_t na, nb, bits_a, bits_b;
+    uint64_t *out;   // na + nb + 1 limbs on the device, fully written
+    int square;
+    int school;
+    ffg_plan pl;
+};
+
+// The plan a method gives one product (methods: include/ffg.h FFG_M_*).
+static int method_plan(int method, uint64_t bits_a, uint64_t bits_b, int square, BJob *j) {
+    const uint64_t la = (bits_a + 63) / 64, lb = (bits_b + 63) / 64, minlen = la < lb ? la : lb;
+    j->school = 0;
+    if (method == FFG_M_PLAIN) {
+        // the reference's thresholds (src/mul_basic.c:30-38, 64-106): schoolbook up to
+        // 64 limbs; the NTT from 200; between them the reference recurses with
+        // Karatsuba down to schoolbook products, which the GPU runs as one
+        // schoolbook product
+        method = minlen >= 200 ? FFG_M_NTT : FFG_M_SCHOOL;
+    }
+    if (method == FFG_M_SCHOOL) {
+        j->school = 1;
+        return FFG_OK;
+    }
+    int rc = plan_select(bits_a, bits_b, square, &j->pl);
+    if (rc || j->pl.split || method == FFG_M_NTT) return rc;
+    if (method != FFG_M_NTT_POW2 && method != FFG_M_NTT_R3) return fail(FFG_E_ARG, "unknown method %d", method);
+    // the same width, the transform length forced to 2^k or 3 2^k
+    ffg_plan q = j->pl;
+    const uint64_t conv = q.conv;
+    uint64_t L = 16;
+    uint32_t lg = 4;
+    while (L < conv) L <<= 1, lg++;
+    if (method == FFG_M_NTT_R3) {
+        uint64_t L3 = 48;
+        uint32_t lg3 = 4;
+        while (L3 < conv) L3 <<= 1, lg3++;
+        L = L3, lg = lg3;
+    }
+    if (L > g.max_L) return FFG_OK; // past the cap: keep the reference's plan
+    q.L = L, q.lg = lg, q.r3 = method == FFG_M_NTT_R3;
+    gpu_geometry(&q);
+    j->pl = q;
+    return FFG_OK;
+}
+
+struct GroupKey {
+    uint32_t kernel, lg, r3, width, row_lg, square;
+    bool operator<(const GroupKey &o) const {
+        return std::tie(kernel, lg, r3, width, row_lg, square) < std::tie(o.kernel, o.lg, o.r3, o.width, o.row_lg, o.square);
+    }
+};
+
+// Runs a batch: one schoolbook launch for every schoolbook product, then per
+// group of products sharing an NTT plan one transform launch set and one CRT
+// launch; split products one by one.  Job records go to the device in one
+// copy.
+static int run_batch(std::vector<BJob> &jobs, cudaStream_t st) {
+    std::vector<SchoolJob> sj;
+    std::map<GroupKey, std::vector<size_t>> groups;
+    std::vector<size_t> splits;
+    double school_bytes = 0;
+    uint32_t school_ctas_max = 0;
+    for (size_t i = 0; i < jobs.size(); i++) {
+        BJob &J = jobs[i];
+        if (J.school) {
+            SchoolJob s{};
+            s.a = J.a, s.b = J.square ? J.a : J.b;
+            s.na = (J.bits_a + 63) / 64, s.nb = J.square ? s.na : (J.bits_b + 63) / 64;
+            s.out = J.out;
+            s.nlimbs = J.na + (J.square ? J.na : J.nb) + 1;
+            s.maps = (uint32_t *)arena_alloc((size_t)school_ctas(s.nlimbs) * 4);
+            if (!s.maps) return fail(FFG_E_NOMEM, "device arena: schoolbook maps");
+            school_ctas_max = std::max(school_ctas_max, school_ctas(s.nlimbs));
+            school_bytes += 8.0 * (double)(s.na + s.nb + s.nlimbs);
+            sj.push_back(s);
+        } else if (J.pl.split) {
+            splits.push_back(i);
+        } else {
+            GroupKey k{J.pl.kernel, J.pl.lg, J.pl.r3, J.pl.width, J.pl.row_lg, (uint32_t)J.square};
+            groups[k].push_back(i);
+        }
+    }
+    // host images of every device job array, packed into one copy
+    std::vector<char> img;
+    auto put = [&](const void *p, size_t n) {
+        size_t off = (img.size() + 255) & ~(size_t)255;
+        img.resize(off + n);
+        memcpy(img.data() + off, p, n);
+        return off;
+    };
+    struct Launch {
+        GroupKey key;
+        size_t conv_off, crt_off, count;
+        uint32_t crt_ctas_max;
+        double conv_bytes, crt_bytes;
+        ffg_plan pl;
+    };
+    std::vector<Launch> launches;
+    size_t school_off = sj.empty() ? 0 : put(sj.data(), sj.size() * sizeof(SchoolJob));
+    for (auto &kv : groups) {
+        const GroupKey &k = kv.first;
+        const ffg_plan &pl = jobs[kv.second[0]].pl;
+        const uint64_t L = pl.L;
+        const uint32_t w = pl.width;
+        std::vector<ConvJob> cj;
+        std::vector<FSJob> fj;
+        std::vector<CrtJob> rj;
+        uint32_t scl[3], scls[3];
+        scale_consts(L, scl, scls);
+        Launch ln{k, 0, 0, kv.second.size(), 0, 0, 0, pl};
+        for (size_t idx : kv.second) {
+            BJob &J = jobs[idx];
+            uint32_t *ya = (uint32_t *)arena_alloc(3 * L * sizeof(uint32_t));
+            uint32_t *yb = J.square ? nullptr : (uint32_t *)arena_alloc(3 * L * sizeof(uint32_t));
+            if (!ya || (!J.square && !yb)) return fail(FFG_E_NOMEM, "device arena: batch residues");
+            const uint64_t ca = (J.bits_a + w - 1) / w, cb = J.square ? ca : (J.bits_b + w - 1) / w;
+            const uint64_t nb = J.square ? J.na : J.nb;
+            if (k.kernel == 0) {
+                ConvJob c{};
+                c.a = J.a, c.b = J.square ? J.a : J.b, c.na = J.na, c.nb = nb, c.ca = ca, c.cb = cb;
+                c.y = ya, c.y_stride = L, c.L_words = (uint32_t)L, c.n = pl.lg, c.r3 = pl.r3, c.width = w;
+                c.square = J.square, c.conv = (uint32_t)(ca + cb - 1);
+                memcpy(c.scl, scl, sizeof scl);
+                memcpy(c.scls, scls, sizeof scls);
+                cj.push_back(c);
+            } else {
+                FSJob f{};
+                f.a = J.a, f.b = J.square ? J.a : J.b, f.na = J.na, f.nb = nb, f.ca = ca, f.cb = cb;
+                f.ya = ya, f.yb = yb, f.width = w;
+                fj.push_back(f);
+            }
+            ln.conv_bytes += 8.0 * (double)(J.na + (J.square ? 0 : nb)) + 12.0 * (double)(ca + cb - 1);
+            CrtJob r{};
+            r.y = ya, r.y_stride = L, r.conv = ca + cb - 1, r.out = J.out, r.nlimbs = J.na + nb + 1, r.width = w;
+            r.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(r.nlimbs, w) * 4);
+            if (!r.maps) return fail(FFG_E_NOMEM, "device arena: batch carry maps");
+            ln.crt_ctas_max = std::max(ln.crt_ctas_max, crt_ctas(r.nlimbs, w));
+            ln.crt_bytes += 12.0 * (double)r.conv + 8.0 * (double)r.nlimbs;
+            rj.push_back(r);
+        }
+        ln.conv_off = k.kernel == 0 ? put(cj.data(), cj.size() * sizeof(ConvJob)) : put(fj.data(), fj.size() * sizeof(FSJob));
+        ln.crt_off = put(rj.data(), rj.size() * sizeof(CrtJob));
+        launches.push_back(ln);
+    }
+    char *dimg = nullptr;
+    if (!img.empty()) {
+        dimg = (char *)arena_alloc(img.size());
+        if (!dimg) return fail(FFG_E_NOMEM, "device arena: batch job records");
+        CK(cudaMemcpyAsync(dimg, img.data(), img.size(), cudaMemcpyHostToDevice, st));
+    }
+    cudaError_t e;
+    for (size_t base = 0; base < sj.size(); base += 65535) {
+        const uint32_t cnt = (uint32_t)std::min<size_t>(65535, sj.size() - base);
+        e = launch_school_batch((const SchoolJob *)(dimg + school_off) + base, cnt, school_ctas_max, st,
+                                school_bytes * cnt / sj.size());
+        if (e) return fail(FFG_E_CUDA, "schoolbook batch: %s", cudaGetErrorString(e));
+    }
+    for (const Launch &ln : launches) {
+        const bool sq = ln.key.square != 0;
+        if (ln.key.kernel == 0) {
+            ConvJobs cjs{};
+            cjs.ext = (const ConvJob *)(dimg + ln.conv_off);
+            e = launch_conv_small(g.P3, cjs, (uint32_t)ln.count, (uint32_t)ln.pl.L, !sq, st, ln.conv_bytes);
+            if (e) return fail(FFG_E_CUDA, "batched one-CTA transforms: %s", cudaGetErrorString(e));
+        } else {
+            FourStep G = four_step_geometry(ln.pl, sq);
+            const size_t per = sq ? 65535 : 32767;
+            for (size_t base = 0; base < ln.count; base += per) {
+                FSJobs fjs{};
+                fjs.ext = (const FSJob *)(dimg + ln.conv_off) + base;
+                const uint32_t cnt = (uint32_t)std::min(per, ln.count - base);
+                e = launch_four_step(g.P3, G, fjs, cnt, st, ln.conv_bytes * cnt / ln.count);
+                if (e) return fail(FFG_E_CUDA, "batched four-step: %s", cudaGetErrorString(e));
+            }
+        }
+        for (size_t base = 0; base < ln.count; base += 65535) {
+            const uint32_t cnt = (uint32_t)std::min<size_t>(65535, ln.count - base);
+            e = launch_crt_batch((const CrtJob *)(dimg + ln.crt_off) + base, cnt, ln.crt_ctas_max, st,
+                                 ln.crt_bytes * cnt / ln.count);
+            if (e) return fail(FFG_E_CUDA, "batched CRT: %s", cudaGetErrorString(e));
+        }
+    }
+    for (size_t idx : splits) {
+        BJob &J = jobs[idx];
+        Prod p{J.a, J.square ? J.a : J.b, J.na, J.square ? J.na : J.nb, J.bits_a, J.square ? J.bits_a : J.bits_b,
+               J.out, 0};
+        int rc = run_split(p, J.square != 0, J.pl, st);
+        if (rc) return rc;
+    }
+    return FFG_OK;
+}
+
 } // namespace ffg
 
 // =================================================================== C ABI
@@ -1153,5 +1351,109 @@ extern "C" int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t n
     C.maps = (uint32_t *)(s + o_maps);
     e = launch_crt(g.P3, C, st);
     if (e) return fail(FFG_E_CUDA, "ffg_mul_device_noalloc crt: %s", cudaGetErrorString(e));
+    return FFG_OK;
+}
+
+extern "C" int ffg_mul_batch_device(ffg_job *jobs, size_t count, void *stream) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!jobs && count) return fail(FFG_E_ARG, "jobs is NULL");
+    cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    std::vector<BJob> bj;
+    bj.reserve(count);
+    for (size_t i = 0; i < count; i++) {
+        ffg_job &u = jobs[i];
+        const uint64_t nb = u.square ? u.na : u.nb, bb = u.square ? u.bits_a : u.bits_b;
+        if (u.bits_a == 0 || bb == 0) {
+            CK(cudaMemsetAsync(u.out, 0, (u.na + nb + 1) * 8, st));
+            continue;
+        }
+        BJob J{u.a, u.square ? u.a : u.b, u.na, nb, u.bits_a, bb, u.out, u.square != 0, 0, {}};
+        rc = method_plan(u.method, u.bits_a, bb, u.square != 0, &J);
+        if (rc) return rc;
+        bj.push_back(J);
+    }
+    return run_batch(bj, st);
+}
+
+extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!jobs && count) return fail(FFG_E_ARG, "jobs is NULL");
+    cudaStream_t st = g.stream;
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    // normalized sizes, one staging image of every operand, one result area
+    std::vector<uint64_t> na(count), nb(count), ba(count), bb(count), aoff(count), boff(count), roff(count);
+    uint64_t in_limbs = 0, out_limbs = 0;
+    for (size_t i = 0; i < count; i++) {
+        ffg_job &u = jobs[i];
+        ba[i] = bits_of(u.a, u.na);
+        bb[i] = u.square ? ba[i] : bits_of(u.b, u.nb);
+        na[i] = std::max<uint64_t>(1, (ba[i] + 63) / 64);
+        nb[i] = std::max<uint64_t>(1, (bb[i] + 63) / 64);
+        aoff[i] = in_limbs;
+        in_limbs += na[i];
+        boff[i] = u.square ? aoff[i] : in_limbs;
+        if (!u.square) in_limbs += nb[i];
+        roff[i] = out_limbs;
+        out_limbs += na[i] + nb[i] + 1;
+    }
+    uint64_t *din = (uint64_t *)arena_alloc(std::max<uint64_t>(1, in_limbs) * 8);
+    uint64_t *dout = (uint64_t *)arena_alloc(std::max<uint64_t>(1, out_limbs) * 8);
+    if (!din || !dout) return fail(FFG_E_NOMEM, "device arena: batch operands");
+    uint64_t *hin = (uint64_t *)pinned_get(std::max<uint64_t>(1, in_limbs) * 8);
+    if (!hin) return fail(FFG_E_NOMEM, "pinned staging");
+    for (size_t i = 0; i < count; i++) {
+        memcpy(hin + aoff[i], jobs[i].a, std::min(na[i], jobs[i].na) * 8);
+        if (na[i] > jobs[i].na) hin[aoff[i]] = 0;
+        if (!jobs[i].square) {
+            memcpy(hin + boff[i], jobs[i].b, std::min(nb[i], jobs[i].nb) * 8);
+            if (nb[i] > jobs[i].nb) hin[boff[i]] = 0;
+        }
+    }
+    CK(cudaMemcpyAsync(din, hin, in_limbs * 8, cudaMemcpyHostToDevice, st));
+    std::vector<BJob> bj;
+    for (size_t i = 0; i < count; i++) {
+        if (ba[i] == 0 || bb[i] == 0) {
+            CK(cudaMemsetAsync(dout + roff[i], 0, (na[i] + nb[i] + 1) * 8, st));
+            continue;
+        }
+        BJob J{din + aoff[i], din + boff[i], na[i], nb[i], ba[i], bb[i], dout + roff[i], jobs[i].square != 0, 0, {}};
+        rc = method_plan(jobs[i].method, ba[i], bb[i], jobs[i].square != 0, &J);
+        if (rc) {
+            pinned_release(hin);
+            return rc;
+        }
+        bj.push_back(J);
+    }
+    rc = run_batch(bj, st);
+    if (rc) {
+        cudaStreamSynchronize(st);
+        pinned_release(hin);
+        return rc;
+    }
+    uint64_t *hout = (uint64_t *)pinned_get(std::max<uint64_t>(1, out_limbs) * 8);
+    if (!hout) {
+        cudaStreamSynchronize(st);
+        pinned_release(hin);
+        return fail(FFG_E_NOMEM, "pinned staging");
+    }
+    CK(cudaMemcpyAsync(hout, dout, out_limbs * 8, cudaMemcpyDeviceToHost, st));
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (!e)
+        for (size_t i = 0; i < count; i++) {
+            uint64_t n = na[i] + nb[i];
+            while (n > 1 && hout[roff[i] + n - 1] == 0) n--;
+            memcpy(jobs[i].out, hout + roff[i], n * 8);
+            jobs[i].nout = n;
+        }
+    pinned_release(hin);
+    pinned_release(hout);
+    if (e) return fail(FFG_E_CUDA, "batch: %s", cudaGetErrorString(e));
     return FFG_OK;
 }

@@ -101,14 +101,34 @@ struct LinJob {
 // a whole chain can be captured into a CUDA graph.
 constexpr int FFG_CONV_JOBS = 2; // one-CTA convolutions per launch
 constexpr int FFG_FS_JOBS = 4;   // four-step products (or split pieces) per launch
+// A launch takes its jobs inline, or -- for batches of any size -- from a
+// device array `ext` (then the inline entries are unused).
 struct ConvJobs {
     ConvJob j[FFG_CONV_JOBS];
+    const ConvJob *ext;
 };
 struct FSJobs {
     FSJob j[FFG_FS_JOBS];
+    const FSJob *ext;
+};
+
+// One schoolbook product out = a b (the reference's big_mul_schoolbook,
+// src/bigint.c:257-276), nlimbs = na + nb (+ slack) limbs fully written.
+struct SchoolJob {
+    const uint64_t *a, *b;
+    uint64_t na, nb;
+    uint64_t *out;
+    uint64_t nlimbs;
+    uint32_t *maps; // school_ctas(nlimbs) words
 };
 
 uint32_t crt_ctas(uint64_t nlimbs, uint32_t width); // CTAs (and carry maps) of one CRT
+__host__ __device__ uint32_t school_ctas(uint64_t nlimbs); // CTAs (and carry maps) of one schoolbook product
+// Batches in device arrays: one launch (plus one settle) for all products.
+cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
+                             double bytes);
+cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
+                                double bytes);
 uint32_t lin_ctas(uint64_t len);                    // CTAs of one linear pass
 
 cudaError_t launch_conv_small(const Primes3 &P3, const ConvJobs &jobs, uint32_t njobs, uint32_t maxL,
@@ -122,7 +142,7 @@ cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st);
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st);
 
 // Kernel families the profiler tracks (ffg_profile_read in include/ffg.h).
-enum ProfKind { PK_CONV_SMALL = 0, PK_COL_FWD, PK_ROW_CONV, PK_COL_INV, PK_CRT, PK_CARRY, PK_LIN, PK_COUNT };
+enum ProfKind { PK_CONV_SMALL = 0, PK_COL_FWD, PK_ROW_CONV, PK_COL_INV, PK_CRT, PK_CARRY, PK_LIN, PK_SCHOOL, PK_COUNT };
 
 // Brackets one kernel launch on stream st with CUDA events when profiling is
 // on, and counts launches always.  bytes: the launch's algorithmic bytes.

@@ -29,6 +29,10 @@ namespace ffg {
 template <typename L, typename T, int N>
 FFG_DEV_INLINE void job_to_smem(const L &list, uint32_t i, T *dst) {
     if (threadIdx.x == 0) {
+        if (list.ext) {
+            *dst = list.ext[i];
+            return;
+        }
 #pragma unroll
         for (int k = 0; k < N; k++)
             if (i == (uint32_t)k) *dst = list.j[k];

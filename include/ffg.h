@@ -72,6 +72,39 @@ int ffg_mul_host(uint64_t *out, size_t *nout, const uint64_t *a, size_t na, cons
 int ffg_mul_device(uint64_t *out, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b, size_t nb,
                    uint64_t bits_b, int square, void *stream);
 
+/* Methods for one product of a batch. */
+enum {
+    FFG_M_PLAIN = -1,   /* the reference's thresholds (src/mul_basic.c:30-38): schoolbook up to
+                           64 limbs, the NTT plan of big_mul_ntt from 200 limbs; the range between,
+                           Karatsuba over schoolbook in the reference, is one schoolbook product */
+    FFG_M_SCHOOL = 0,   /* schoolbook (big_mul_schoolbook, src/bigint.c:257-276) */
+    FFG_M_NTT = 1,      /* big_mul_ntt's plan (src/mul_ntt.c:97-118), the split past the cap */
+    FFG_M_NTT_POW2 = 2, /* the same width, the transform length forced to 2^k */
+    FFG_M_NTT_R3 = 3    /* the same width, the transform length forced to 3 * 2^k */
+};
+
+/* One product of a batch.  Device variant: a, b, out device pointers, out
+   holds na + nb + 1 limbs and is fully written, bits_* are bit lengths (upper
+   bounds allowed).  Host variant: host pointers, out holds na + nb limbs,
+   bits_* ignored, the normalized length comes back in nout. */
+typedef struct {
+    const uint64_t *a, *b;
+    uint64_t na, nb;
+    uint64_t bits_a, bits_b;
+    uint64_t *out;
+    uint64_t nout;
+    int32_t square;
+    int32_t method;
+} ffg_job;
+
+/* A batch of independent products in as few launches as their plans allow:
+   every schoolbook product in one launch, every group of products sharing
+   an NTT plan in one launch set and one CRT launch (the reference multiplies
+   them one by one, e.g. the products of one decimal level,
+   src/decimal.c:177-203). */
+int ffg_mul_batch_device(ffg_job *jobs, size_t count, void *stream);
+int ffg_mul_batch_host(ffg_job *jobs, size_t count);
+
 /* No counterpart in the reference.  ffg_mul_device without any device
    allocation, for callers that cannot allocate once running: code issuing
    work while a CUDA graph is being captured, frameworks whose allocator owns
@@ -110,7 +143,7 @@ int ffg_set_device(int device);
    launches, summed device milliseconds and summed algorithmic bytes since
    ffg_profile() was last called.  Families: 0 one-CTA convolution, 1 forward
    column pass, 2 row pass (forward, pointwise, inverse), 3 inverse column
-   pass, 4 CRT, 5 carry settle, 6 linear pass. */
+   pass, 4 CRT, 5 carry settle, 6 linear pass, 7 schoolbook. */
 void ffg_profile(uint32_t family_mask); /* bit k on: bracket family k; 0: off */
 int ffg_profile_read(int kind, uint64_t *launches, double *ms, double *bytes);
 /* Kernel launches made by the library since it was loaded. */
