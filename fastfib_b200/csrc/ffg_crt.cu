@@ -141,51 +141,61 @@ FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t ct
     if (threadIdx.x == 0) J.maps[cta] = map;
 }
 
-// Carries between CTAs: one warp per 32 CTAs composes the maps of every CTA
-// before them (from carry 0 into the first), then each lane whose CTA
-// receives a carry adds it into that CTA's lowest limbs.
-FFG_DEV_INLINE void settle_warp(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *__restrict__ maps,
-                                uint32_t ncta, uint32_t group);
+// Carries between CTAs: one block of SETTLE_THREADS threads per product.
+// Thread t composes the maps of its run of consecutive CTAs, a block-wide
+// scan of those composites gives the carry into every run (carry 0 into the
+// first CTA), and each thread walks its run again adding the carry into the
+// CTAs that receive one (a carry stops at the first limb that does not wrap).
+constexpr uint32_t SETTLE_THREADS = 1024;
 
-__global__ void __launch_bounds__(32) k_settle(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs,
-                                               const uint32_t *__restrict__ maps, uint32_t ncta) {
-    settle_warp(out, nlimbs, cta_limbs, maps, ncta, blockIdx.x);
+FFG_DEV_INLINE void settle_block(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *__restrict__ maps,
+                                 uint32_t ncta) {
+    __shared__ uint32_t wpre[SETTLE_THREADS / 32];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t per = (ncta + SETTLE_THREADS - 1) / SETTLE_THREADS;
+    const uint32_t q0 = min(ncta, threadIdx.x * per), q1 = min(ncta, q0 + per);
+    uint32_t run = 2u; // identity: c -> c
+    for (uint32_t q = q0; q < q1; q++) run = map_then(run, maps[q]);
+    const uint32_t inc = warp_map_scan(run);
+    if (lane == 31) wpre[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t v = warp_map_scan(wpre[lane]); // SETTLE_THREADS / 32 == 32 warps
+        __syncwarp();
+        wpre[lane] = v;
+    }
+    __syncthreads();
+    uint32_t exc = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) exc = 2u;
+    const uint32_t before = warp ? map_then(wpre[warp - 1], exc) : exc;
+    uint32_t carry = map_apply(before, 0);
+    for (uint32_t q = q0; q < q1; q++) {
+        if (carry) {
+            const uint64_t end = min(nlimbs, (uint64_t)(q + 1) * cta_limbs);
+            for (uint64_t j = (uint64_t)q * cta_limbs; j < end; j++)
+                if (++out[j] != 0) break;
+        }
+        carry = map_apply(maps[q], carry);
+    }
+}
+
+__global__ void __launch_bounds__(SETTLE_THREADS) k_settle(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs,
+                                                           const uint32_t *__restrict__ maps, uint32_t ncta) {
+    settle_block(out, nlimbs, cta_limbs, maps, ncta);
 }
 
 // Settles a batch of CRTs (blockIdx.y the product).
-__global__ void __launch_bounds__(32) k_settle_crt_batch(const CrtJob *__restrict__ jobs) {
+__global__ void __launch_bounds__(SETTLE_THREADS) k_settle_crt_batch(const CrtJob *__restrict__ jobs) {
     const CrtJob J = jobs[blockIdx.y];
     const uint32_t ncta = crt_ctas_dev(J.nlimbs, J.width);
-    if (ncta <= 1 || blockIdx.x * 32 >= ncta) return;
-    settle_warp(J.out, J.nlimbs, CRT_NL_PER_W * J.width, J.maps, ncta, blockIdx.x);
-}
-
-FFG_DEV_INLINE void settle_warp(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *__restrict__ maps,
-                                uint32_t ncta, uint32_t group) {
-    const uint32_t lane = threadIdx.x, first = group * 32;
-    uint32_t carry = 0;
-    for (uint32_t base = 0; base < first; base += 32) {
-        const uint32_t m = maps[base + lane]; // base + 32 <= first <= ncta
-        const uint32_t inc = warp_map_scan(m);
-        carry = map_apply(__shfl_sync(0xffffffffu, inc, 31), carry);
-    }
-    const uint32_t q = first + lane;
-    const uint32_t m = q < ncta ? maps[q] : 2u;
-    const uint32_t inc = warp_map_scan(m);
-    uint32_t exc = __shfl_up_sync(0xffffffffu, inc, 1);
-    if (lane == 0) exc = 2u;
-    const uint32_t c = map_apply(exc, carry);
-    if (q < ncta && c) {
-        const uint64_t end = min(nlimbs, (uint64_t)(q + 1) * cta_limbs);
-        for (uint64_t j = (uint64_t)q * cta_limbs; j < end; j++)
-            if (++out[j] != 0) break;
-    }
+    if (ncta <= 1) return;
+    settle_block(J.out, J.nlimbs, CRT_NL_PER_W * J.width, J.maps, ncta);
 }
 
 static cudaError_t launch_settle(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *maps,
                                  uint32_t ncta, cudaStream_t st) {
     if (ncta <= 1) return cudaSuccess; // nothing comes into the first CTA
-    k_settle<<<(ncta + 31) / 32, 32, 0, st>>>(out, nlimbs, cta_limbs, maps, ncta);
+    k_settle<<<1, SETTLE_THREADS, 0, st>>>(out, nlimbs, cta_limbs, maps, ncta);
     return cudaGetLastError();
 }
 
@@ -234,7 +244,7 @@ cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_
     cudaError_t e = cudaGetLastError();
     if (e || max_ctas <= 1) return e;
     prof_begin(PK_CARRY, st);
-    k_settle_crt_batch<<<dim3((max_ctas + 31) / 32, count), 32, 0, st>>>(d_jobs);
+    k_settle_crt_batch<<<dim3(1, count), SETTLE_THREADS, 0, st>>>(d_jobs);
     prof_end(PK_CARRY, st, 4.0 * max_ctas * count);
     return cudaGetLastError();
 }
@@ -305,11 +315,11 @@ __global__ void __launch_bounds__(SCHOOL_THREADS) k_school(const SchoolJob *__re
     if (threadIdx.x == 0) J.maps[blockIdx.x] = map;
 }
 
-__global__ void __launch_bounds__(32) k_settle_school_batch(const SchoolJob *__restrict__ jobs) {
+__global__ void __launch_bounds__(SETTLE_THREADS) k_settle_school_batch(const SchoolJob *__restrict__ jobs) {
     const SchoolJob J = jobs[blockIdx.y];
     const uint32_t ncta = school_ctas(J.nlimbs);
-    if (ncta <= 1 || blockIdx.x * 32 >= ncta) return;
-    settle_warp(J.out, J.nlimbs, SCHOOL_NL, J.maps, ncta, blockIdx.x);
+    if (ncta <= 1) return;
+    settle_block(J.out, J.nlimbs, SCHOOL_NL, J.maps, ncta);
 }
 
 cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
@@ -321,7 +331,7 @@ cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_
     cudaError_t e = cudaGetLastError();
     if (e || max_ctas <= 1) return e;
     prof_begin(PK_CARRY, st);
-    k_settle_school_batch<<<dim3((max_ctas + 31) / 32, count), 32, 0, st>>>(d_jobs);
+    k_settle_school_batch<<<dim3(1, count), SETTLE_THREADS, 0, st>>>(d_jobs);
     prof_end(PK_CARRY, st, 4.0 * max_ctas * count);
     return cudaGetLastError();
 }

@@ -164,31 +164,65 @@ static int fail(int code, const char *fmt, ...) {
                                            __FILE__, __LINE__);                                      \
     } while (0)
 
-// Device tables for the three primes (see PrimeDev).
+// The (stride 2^sl, radix 2^M) pairs the line schedules use, with sl > 0
+// (steps at stride 1 need no twiddles), and their table offsets.
+static size_t step_table_layout(uint32_t *off) {
+    for (int k = 0; k < 15 * 6; k++) off[k] = ~0u;
+    size_t total = 0;
+    for (uint32_t n = 1; n <= (uint32_t)FFG_LINE_LG; n++) {
+        int m[4], sl[4];
+        const int k = schedule(n, m, sl);
+        for (int i = 0; i < k; i++) {
+            if (!sl[i] || off[sl[i] * 6 + m[i]] != ~0u) continue;
+            off[sl[i] * 6 + m[i]] = (uint32_t)total;
+            total += (((size_t)1 << m[i]) - 1) << sl[i];
+        }
+    }
+    return total;
+}
+
+static uint32_t brev_bits(uint32_t x, int bits) {
+    uint32_t r = 0;
+    for (int b = 0; b < bits; b++) r |= ((x >> b) & 1u) << (bits - 1 - b);
+    return r;
+}
+
+// Device tables for the three primes (see PrimeDev) and the constant-memory
+// roots of the line transforms (LineConsts).
 static int build_tables() {
-    const size_t nrt = (size_t)1 << FFG_LINE_LG, nr3 = (size_t)1 << kR3TabLg;
+    LineConsts lc{};
+    const size_t nstw = step_table_layout(lc.tw_off), nr3 = (size_t)1 << kR3TabLg;
     const size_t ntwh = (size_t)(FFG_M / FFG_TW_LO);
-    const size_t per = nrt * 2 * sizeof(uint2) + nr3 * 2 * sizeof(uint4) + (FFG_TW_LO + ntwh) * sizeof(uint32_t);
+    const size_t per = nstw * 2 * sizeof(uint2) + nr3 * 2 * sizeof(uint4) + (FFG_TW_LO + ntwh) * sizeof(uint32_t);
     std::vector<char> host(per * 3);
     CK(cudaMalloc(&g.tables, per * 3));
     for (int k = 0; k < 3; k++) {
         const uint32_t p = kP[k], gen = kG[k];
         char *hb = host.data() + per * k;
         char *db = (char *)g.tables + per * k;
-        uint2 *rt = (uint2 *)hb, *irt = rt + nrt;
-        uint4 *r3f = (uint4 *)(irt + nrt), *r3i = r3f + nr3;
+        uint2 *stw = (uint2 *)hb, *istw = stw + nstw;
+        uint4 *r3f = (uint4 *)(istw + nstw), *r3i = r3f + nr3;
         uint32_t *twl = (uint32_t *)(r3i + nr3), *twh = twl + FFG_TW_LO;
-        rt[0] = irt[0] = make_uint2(0, 0);
-        for (size_t h = 1; h < nrt; h <<= 1) {
-            uint32_t w = powmod(gen, (p - 1) / (2 * h), p), wi = inv_mod(w, p);
-            uint32_t c = 1, ci = 1;
-            for (size_t i = 0; i < h; i++) {
-                rt[h + i] = make_uint2(c, shoup_q(c, p));
-                irt[h + i] = make_uint2(ci, shoup_q(ci, p));
-                c = mulm(c, w, p);
-                ci = mulm(ci, wi, p);
+        // step twiddles: slot t of group j at stride S = 2^sl, radix 2^M gets
+        // ω_N^(j brev_M(t)), N = 2^M S, at (t - 1) S + j
+        for (int sl = 1; sl < 15; sl++)
+            for (int M = 1; M <= 5; M++) {
+                const uint32_t o = lc.tw_off[sl * 6 + M];
+                if (o == ~0u) continue;
+                const uint64_t S = (uint64_t)1 << sl, N = S << M;
+                const uint32_t wN = powmod(gen, (p - 1) / N, p), wNi = inv_mod(wN, p);
+                for (uint32_t t = 1; t < (1u << M); t++) {
+                    const uint32_t e = brev_bits(t, M);
+                    const uint32_t a = powmod(wN, e, p), ai = powmod(wNi, e, p);
+                    uint32_t c = 1, ci = 1;
+                    for (uint64_t j = 0; j < S; j++) {
+                        stw[o + (t - 1) * S + j] = make_uint2(c, shoup_q(c, p));
+                        istw[o + (t - 1) * S + j] = make_uint2(ci, shoup_q(ci, p));
+                        c = mulm(c, a, p);
+                        ci = mulm(ci, ai, p);
+                    }
+                }
             }
-        }
         r3f[0] = r3i[0] = make_uint4(0, 0, 0, 0);
         for (int n = 0; n < kR3TabLg; n++) {
             const uint64_t B = (uint64_t)1 << n, R = 3 * B;
@@ -219,14 +253,27 @@ static int build_tables() {
         P.v3s = shoup_q(P.v3, p);
         P.c32 = (uint32_t)((1ull << 32) % p);
         P.c32s = shoup_q(P.c32, p);
-        P.rt = (const uint2 *)db;
-        P.irt = P.rt + nrt;
-        P.r3f = (const uint4 *)(P.irt + nrt);
+        P.stw = (const uint2 *)db;
+        P.istw = P.stw + nstw;
+        P.r3f = (const uint4 *)(P.istw + nstw);
         P.r3i = P.r3f + nr3;
         P.twl = (const uint32_t *)(P.r3i + nr3);
         P.twh = P.twl + FFG_TW_LO;
+
+        const uint32_t w32 = powmod(gen, (p - 1) / 32, p), w32i = inv_mod(w32, p);
+        uint32_t f = 1, fi = 1;
+        for (int e = 0; e < 16; e++) {
+            lc.f[k][e] = make_uint2(f, shoup_q(f, p));
+            lc.i[k][e] = make_uint2(fi, shoup_q(fi, p));
+            f = mulm(f, w32, p);
+            fi = mulm(fi, w32i, p);
+        }
+        lc.w3[k] = make_uint2(P.w3, P.w3s);
+        lc.v3[k] = make_uint2(P.v3, P.v3s);
+        lc.pinv[k] = P.pinv;
     }
     CK(cudaMemcpy(g.tables, host.data(), per * 3, cudaMemcpyHostToDevice));
+    CK(set_line_consts(lc));
     return FFG_OK;
 }
 
@@ -413,6 +460,7 @@ static FourStep four_step_geometry(const ffg_plan &pl, bool square) {
     while (wc & (wc - 1)) wc &= wc - 1;
     if (wc > (1u << G.c)) wc = 1u << G.c;
     G.wc = wc;
+    G.wc_lg = (uint32_t)__builtin_ctz(wc);
     G.col_stride = line_stride(G.R);
     G.square = square;
     G.mode = ROW_CONV;

@@ -42,7 +42,7 @@ struct FourStep {
     uint64_t L;             // transform length = R * 2^c
     uint32_t c;             // log2 of the row length C
     uint32_t R, rn, r3;     // column length R = 3^r3 2^rn
-    uint32_t wc;            // columns per CTA in the column passes
+    uint32_t wc, wc_lg;     // columns per CTA in the column passes (a power of 2 dividing 256)
     uint32_t col_stride;    // shared words per column line
     uint32_t square;
     uint32_t mode;          // RowMode of k_row_conv
@@ -131,6 +131,7 @@ cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_
                                 double bytes);
 uint32_t lin_ctas(uint64_t len);                    // CTAs of one linear pass
 
+cudaError_t set_line_consts(const LineConsts &h); // once, before any transform
 cudaError_t launch_conv_small(const Primes3 &P3, const ConvJobs &jobs, uint32_t njobs, uint32_t maxL,
                               bool any_distinct, cudaStream_t st, double bytes);
 cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t njobs,

@@ -18,8 +18,8 @@
 // The reference's top radix-16 passes over column chunks and in-cache
 // sub-blocks (src/ntt_conv.c:158-226) play the same roles on the CPU; here
 // each pass is one HBM round trip of the residues.
-#include "ffg_device.cuh"
 #include "ffg_internal.h"
+#include "ffg_lines.cuh"
 
 namespace ffg {
 
@@ -39,169 +39,193 @@ FFG_DEV_INLINE void job_to_smem(const L &list, uint32_t i, T *dst) {
     }
 }
 
+cudaError_t set_line_consts(const LineConsts &h) { return cudaMemcpyToSymbol(c_lines, &h, sizeof h); }
+
+// Calls body<PI>(...) for the CTA's prime (blockIdx.y), so each prime's
+// constants are compile-time inside the body.
+#define FFG_PRIME_DISPATCH(body, ...)                                                                  \
+    switch (blockIdx.y) {                                                                            \
+    case 0: body<0>(P3.pr[0], __VA_ARGS__); break;                                                   \
+    case 1: body<1>(P3.pr[1], __VA_ARGS__); break;                                                   \
+    default: body<2>(P3.pr[2], __VA_ARGS__); break;                                                  \
+    }
+
 // ------------------------------------------------------------ short lengths
 
-__global__ void __launch_bounds__(256, 3) k_conv_small(Primes3 P3, ConvJobs jobs) {
-    extern __shared__ uint32_t smem[];
-    __shared__ ConvJob J;
-    job_to_smem<ConvJobs, ConvJob, FFG_CONV_JOBS>(jobs, blockIdx.x, &J);
-    __syncthreads();
-    const PrimeDev P = P3.pr[blockIdx.y];
-    const uint32_t L = J.L_words, p = P.p;
-    const uint32_t stride = line_stride(L);
+template <int PI>
+FFG_DEV_INLINE void conv_small_body(const PrimeDev &P, const ConvJob &J, uint32_t *smem) {
+    const uint32_t L = J.L_words, stride = line_stride(L);
     uint32_t *fa = smem, *fb = smem + stride;
     const bool sq = J.square != 0;
-
-    for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) {
+    for (uint32_t i = threadIdx.x; i < L; i += kLineThreads) {
         fa[pad_idx(i)] = i < J.ca ? reduce_digit(digit_at(J.a, J.na, i, J.width), P) : 0;
         if (!sq) fb[pad_idx(i)] = i < J.cb ? reduce_digit(digit_at(J.b, J.nb, i, J.width), P) : 0;
     }
     __syncthreads();
-    LineSet ls{sq ? 1u : 2u, J.n, J.r3, stride};
-    lines_forward(smem, ls, P);
-    for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) {
-        uint32_t x = fa[pad_idx(i)];
-        fa[pad_idx(i)] = mont(x, sq ? x : fb[pad_idx(i)], p, P.pinv);
+    lines_fwd<PI>(smem, sq ? 0 : 1, J.n, J.r3, stride, P);
+    for (uint32_t i = threadIdx.x; i < L; i += kLineThreads) {
+        const uint32_t x = fa[pad_idx(i)];
+        fa[pad_idx(i)] = mo<PI>(x, sq ? x : fb[pad_idx(i)]);
     }
     __syncthreads();
-    ls.lines = 1;
-    lines_inverse(smem, ls, P);
-    const uint32_t scl = J.scl[blockIdx.y], scls = J.scls[blockIdx.y];
-    uint32_t *y = J.y + (size_t)blockIdx.y * J.y_stride;
-    for (uint32_t i = threadIdx.x; i < J.conv; i += blockDim.x) y[i] = shoup(fa[pad_idx(i)], scl, scls, p);
+    lines_inv<PI>(smem, 0, J.n, J.r3, stride, P);
+    const uint2 sc = make_uint2(J.scl[PI], J.scls[PI]);
+    uint32_t *y = J.y + (size_t)PI * J.y_stride;
+    for (uint32_t i = threadIdx.x; i < J.conv; i += kLineThreads) y[i] = sh<PI>(fa[pad_idx(i)], sc);
+}
+
+__global__ void __launch_bounds__(kLineThreads, kLineMinBlocks) k_conv_small(Primes3 P3, ConvJobs jobs) {
+    extern __shared__ uint32_t smem[];
+    __shared__ ConvJob J;
+    job_to_smem<ConvJobs, ConvJob, FFG_CONV_JOBS>(jobs, blockIdx.x, &J);
+    __syncthreads();
+    FFG_PRIME_DISPATCH(conv_small_body, J, smem)
 }
 
 // ------------------------------------------------------------- four-step
+//
+// Column tiles: a CTA holds columns [c0, c0 + wc) of all R rows, wc lines of
+// length R.  In the load and store loops thread t serves column t mod wc and
+// rows t / wc + m (256 / wc), so a warp touches 32 / wc rows of wc
+// consecutive words each.
 
-// Column tile: columns [c0, c0 + wc) of all R rows, wc lines of length R.
-__global__ void __launch_bounds__(256, 3) k_col_fwd(Primes3 P3, FourStep G, FSJobs jobs) {
-    extern __shared__ uint32_t smem[];
-    const uint32_t z = blockIdx.z, op = G.square ? 0 : (z & 1), jb = G.square ? z : (z >> 1);
-    __shared__ FSJob J;
-    job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, jb, &J);
-    __syncthreads();
-    const PrimeDev P = P3.pr[blockIdx.y];
-    const uint32_t R = G.R, C = 1u << G.c, wc = G.wc, stride = G.col_stride;
+// Position holding frequency k1 after the forward column transform.
+FFG_DEV_INLINE uint32_t pos_of(uint32_t k1, uint32_t n, uint32_t r3) {
+    if (!r3) return n ? __brev(k1) >> (32 - n) : 0;
+    const uint32_t q = k1 % 3, i = k1 / 3;
+    return (q << n) + (n ? __brev(i) >> (32 - n) : 0);
+}
+
+template <int PI>
+FFG_DEV_INLINE void col_fwd_body(const PrimeDev &P, const FourStep &G, const FSJob &J, uint32_t *smem) {
+    const uint32_t z = blockIdx.z, op = G.square ? 0 : (z & 1);
+    const uint32_t R = G.R, C = 1u << G.c, wc = G.wc, wlg = G.wc_lg, stride = G.col_stride;
     const uint32_t c0 = blockIdx.x * wc;
     const uint64_t *src = op ? J.b : J.a;
     const uint64_t ns = op ? J.nb : J.na, cs = op ? J.cb : J.ca, off = op ? J.off_b : J.off_a;
-
-    for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
-        uint32_t n1 = idx / wc, c = idx % wc;
-        uint64_t i = (uint64_t)n1 * C + c0 + c;
-        smem[c * stride + pad_idx(n1)] = i < cs ? reduce_digit(digit_at(src, ns, off + i, J.width), P) : 0;
-    }
+    const uint32_t c = threadIdx.x & (wc - 1), r0 = threadIdx.x >> wlg, dr = kLineThreads >> wlg;
+    uint32_t *col = smem + c * stride;
+    tile_digits<PI, 8>(smem, stride, src, ns, cs, off, J.width, C, R, c0, wlg, P);
     __syncthreads();
-    LineSet ls{wc, G.rn, G.r3, stride};
-    lines_forward(smem, ls, P);
-    uint32_t *y = (op ? J.yb : J.ya) + (size_t)blockIdx.y * G.L;
-    for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
-        uint32_t pos = idx / wc, c = idx % wc;
-        uint32_t k1 = freq_of(pos, G.rn, G.r3), n2 = c0 + c;
-        uint64_t E = (uint64_t)n2 * k1 * G.mstep;
-        uint32_t v = smem[c * stride + pad_idx(pos)];
-        y[(size_t)pos * C + n2] = mont(v, tw_mont(P, E), P.p, P.pinv);
+    lines_fwd<PI>(smem, wlg, G.rn, G.r3, stride, P);
+    // twiddle ω_L^(n2 k1) for k1 = r0 + m dr: a running Montgomery product
+    const uint32_t n2 = c0 + c;
+    uint32_t cur = twm<PI>(P, (uint64_t)n2 * r0 % G.L * G.mstep);
+    const uint32_t step = twm<PI>(P, (uint64_t)n2 * dr % G.L * G.mstep);
+    uint32_t *y = (op ? J.yb : J.ya) + (size_t)PI * G.L + n2;
+    for (uint32_t k1 = r0; k1 < R; k1 += dr) {
+        const uint32_t pos = pos_of(k1, G.rn, G.r3);
+        y[(size_t)pos * C] = mo<PI>(col[pad_idx(pos)], cur);
+        cur = mo<PI>(cur, step);
     }
+}
+
+__global__ void __launch_bounds__(kLineThreads, kLineMinBlocks) k_col_fwd(Primes3 P3, FourStep G, FSJobs jobs) {
+    extern __shared__ uint32_t smem[];
+    __shared__ FSJob J;
+    job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, G.square ? blockIdx.z : (blockIdx.z >> 1), &J);
+    __syncthreads();
+    FFG_PRIME_DISPATCH(col_fwd_body, G, J, smem)
 }
 
 // One row (position pos of the column transform) per CTA.  ROW_CONV: forward
 // transform of the row of both operands, pointwise product, inverse.
 // ROW_FWD: forward transform only (the split's pieces).  ROW_ACC_INV: the
 // split's output piece m, sum over i + j = m of A_i B_j on this row
-// (src/mul_split.c:62-78), then the inverse.
-__global__ void __launch_bounds__(256, 3) k_row_conv(Primes3 P3, FourStep G, FSJobs jobs) {
-    extern __shared__ uint32_t smem[];
-    __shared__ FSJob J;
-    job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, blockIdx.z, &J);
-    __syncthreads();
-    const PrimeDev P = P3.pr[blockIdx.y];
-    const uint32_t C = 1u << G.c, pos = blockIdx.x, p = P.p;
+// (src/mul_split.c:62-78), then the inverse.  The inverse rows end with the
+// twiddle ω_L^-(n2 k1), a running product along the row.
+template <int PI>
+FFG_DEV_INLINE void row_body(const PrimeDev &P, const FourStep &G, const FSJob &J, uint32_t *smem) {
+    const uint32_t C = 1u << G.c, pos = blockIdx.x;
     const uint32_t stride = line_stride(C);
     const bool sq = G.square != 0;
-    uint32_t *ya = J.ya + (size_t)blockIdx.y * G.L + (size_t)pos * C;
-    const uint32_t *yb = sq ? ya : J.yb + (size_t)blockIdx.y * G.L + (size_t)pos * C;
+    const size_t rowoff = (size_t)PI * G.L + (size_t)pos * C;
+    uint32_t *ya = J.ya + rowoff;
+    uint32_t *yb = sq ? ya : J.yb + rowoff;
     uint32_t *fa = smem, *fb = smem + stride;
 
     if (G.mode == ROW_ACC_INV) {
-        const uint64_t rowoff = (size_t)blockIdx.y * G.L + (size_t)pos * C;
         const uint32_t m = J.m;
         const uint32_t i0 = m + 1 > J.kb ? m + 1 - J.kb : 0;
         uint32_t i1 = m < J.ka - 1 ? m : J.ka - 1;
         if (J.psq && i1 > m / 2) i1 = m / 2;
-        for (uint32_t t = threadIdx.x; t < C; t += blockDim.x) {
+        for (uint32_t t = threadIdx.x; t < C; t += kLineThreads) {
             uint32_t acc = 0;
             for (uint32_t i = i0; i <= i1; i++) {
                 const uint32_t j = m - i;
-                uint32_t v = mont(J.pa[i * J.piece_stride + rowoff + t], J.pb[j * J.piece_stride + rowoff + t], p,
-                                  P.pinv);
-                acc = add_mod(acc, v, p);
-                if (J.psq && i < j) acc = add_mod(acc, v, p);
+                const uint32_t v = mo<PI>(J.pa[i * J.piece_stride + rowoff + t], J.pb[j * J.piece_stride + rowoff + t]);
+                acc = ad<PI>(acc, v);
+                if (J.psq && i < j) acc = ad<PI>(acc, v);
             }
             fa[pad_idx(t)] = acc;
         }
         __syncthreads();
     } else {
-        for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
-            fa[pad_idx(i)] = ya[i];
-            if (!sq) fb[pad_idx(i)] = yb[i];
-        }
+        line_load<8>(fa, ya, C);
+        if (!sq) line_load<8>(fb, yb, C);
         __syncthreads();
-        LineSet lf{sq ? 1u : 2u, G.c, 0, stride};
-        lines_forward(smem, lf, P);
+        lines_fwd<PI>(smem, sq ? 0 : 1, G.c, 0, stride, P);
         if (G.mode == ROW_FWD) {
-            for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
+            for (uint32_t i = threadIdx.x; i < C; i += kLineThreads) {
                 ya[i] = fa[pad_idx(i)];
-                if (!sq) ((uint32_t *)yb)[i] = fb[pad_idx(i)];
+                if (!sq) yb[i] = fb[pad_idx(i)];
             }
             return;
         }
-        for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
-            uint32_t x = fa[pad_idx(i)];
-            fa[pad_idx(i)] = mont(x, sq ? x : fb[pad_idx(i)], p, P.pinv);
+        for (uint32_t i = threadIdx.x; i < C; i += kLineThreads) {
+            const uint32_t x = fa[pad_idx(i)];
+            fa[pad_idx(i)] = mo<PI>(x, sq ? x : fb[pad_idx(i)]);
         }
         __syncthreads();
     }
-    LineSet ls{1u, G.c, 0, stride};
-    lines_inverse(smem, ls, P);
+    lines_inv<PI>(smem, 0, G.c, 0, stride, P);
     const uint32_t k1 = freq_of(pos, G.rn, G.r3);
-    for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
-        uint64_t E = (uint64_t)i * k1 * G.mstep;
-        E = E ? FFG_M - E : 0; // ω^-e = ω^(M - E)
-        ya[i] = mont(fa[pad_idx(i)], tw_mont(P, E), p, P.pinv);
+    // ω^-e = ω^(M - E); exponents reduced mod L first
+    const uint64_t e0 = (uint64_t)threadIdx.x * k1 % G.L * G.mstep, e1 = (uint64_t)kLineThreads * k1 % G.L * G.mstep;
+    uint32_t cur = twm<PI>(P, e0 ? FFG_M - e0 : 0);
+    const uint32_t step = twm<PI>(P, e1 ? FFG_M - e1 : 0);
+    for (uint32_t i = threadIdx.x; i < C; i += kLineThreads) {
+        ya[i] = mo<PI>(fa[pad_idx(i)], cur);
+        cur = mo<PI>(cur, step);
     }
 }
 
-__global__ void __launch_bounds__(256, 3) k_col_inv(Primes3 P3, FourStep G, FSJobs jobs) {
+__global__ void __launch_bounds__(kLineThreads, kLineMinBlocks) k_row_conv(Primes3 P3, FourStep G, FSJobs jobs) {
     extern __shared__ uint32_t smem[];
     __shared__ FSJob J;
     job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, blockIdx.z, &J);
     __syncthreads();
-    const PrimeDev P = P3.pr[blockIdx.y];
-    const uint32_t R = G.R, C = 1u << G.c, wc = G.wc, stride = G.col_stride;
-    const uint32_t c0 = blockIdx.x * wc;
-    uint32_t *y = J.ya + (size_t)blockIdx.y * G.L;
+    FFG_PRIME_DISPATCH(row_body, G, J, smem)
+}
 
-    for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
-        uint32_t pos = idx / wc, c = idx % wc;
-        smem[c * stride + pad_idx(pos)] = y[(size_t)pos * C + c0 + c];
-    }
+template <int PI>
+FFG_DEV_INLINE void col_inv_body(const PrimeDev &P, const FourStep &G, const FSJob &J, uint32_t *smem) {
+    const uint32_t R = G.R, C = 1u << G.c, wc = G.wc, wlg = G.wc_lg, stride = G.col_stride;
+    const uint32_t c0 = blockIdx.x * wc;
+    const uint32_t c = threadIdx.x & (wc - 1), r0 = threadIdx.x >> wlg, dr = kLineThreads >> wlg;
+    uint32_t *col = smem + c * stride;
+    uint32_t *y = J.ya + (size_t)PI * G.L + c0 + c;
+    tile_load<8>(smem, stride, J.ya + (size_t)PI * G.L + c0, C, R, wlg);
     __syncthreads();
-    LineSet ls{wc, G.rn, G.r3, stride};
-    lines_inverse(smem, ls, P);
-    const uint32_t scl = G.scl[blockIdx.y], scls = G.scls[blockIdx.y];
+    lines_inv<PI>(smem, wlg, G.rn, G.r3, stride, P);
+    const uint2 sc = make_uint2(G.scl[PI], G.scls[PI]);
     if (J.yacc) { // overlap-add of a split output piece
-        uint32_t *acc = J.yacc + (size_t)blockIdx.y * J.acc_stride + J.acc_off;
-        for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
-            uint32_t n1 = idx / wc, c = idx % wc;
-            const size_t at = (size_t)n1 * C + c0 + c;
-            acc[at] = add_mod(acc[at], shoup(smem[c * stride + pad_idx(n1)], scl, scls, P.p), P.p);
+        uint32_t *acc = J.yacc + (size_t)PI * J.acc_stride + J.acc_off + c0 + c;
+        for (uint32_t n1 = r0; n1 < R; n1 += dr) {
+            const size_t at = (size_t)n1 * C;
+            acc[at] = ad<PI>(acc[at], sh<PI>(col[pad_idx(n1)], sc));
         }
         return;
     }
-    for (uint32_t idx = threadIdx.x; idx < R * wc; idx += blockDim.x) {
-        uint32_t n1 = idx / wc, c = idx % wc;
-        y[(size_t)n1 * C + c0 + c] = shoup(smem[c * stride + pad_idx(n1)], scl, scls, P.p);
-    }
+    for (uint32_t n1 = r0; n1 < R; n1 += dr) y[(size_t)n1 * C] = sh<PI>(col[pad_idx(n1)], sc);
+}
+
+__global__ void __launch_bounds__(kLineThreads, kLineMinBlocks) k_col_inv(Primes3 P3, FourStep G, FSJobs jobs) {
+    extern __shared__ uint32_t smem[];
+    __shared__ FSJob J;
+    job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, blockIdx.z, &J);
+    __syncthreads();
+    FFG_PRIME_DISPATCH(col_inv_body, G, J, smem)
 }
 
 // ---------------------------------------------------------------- launchers
