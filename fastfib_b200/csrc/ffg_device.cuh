@@ -101,13 +101,13 @@ FFG_DEV_INLINE void bf_dit(uint32_t &x, uint32_t &y, uint2 w, uint32_t p) {
     x = add_mod(x, t, p);
 }
 
-// The step schedule of a 2^n block: radix-16 steps while more than 10 levels
-// remain (stride >= 64), then one step down to stride 32, then the last step
-// on contiguous groups (stride 1).  Returns the number of steps; step i has
+// The step schedule of a 2^n block: radix-16 steps while more than 9 levels
+// remain (stride >= 32), then one step down to stride 32, then the last step
+// on contiguous groups (stride 1, radix up to 32, no twiddles).  Returns the number of steps; step i has
 // radix 2^m[i] and stride 2^sl[i], listed in DIF order (largest stride first).
 __host__ __device__ inline int schedule(uint32_t n, int (&m)[4], int (&sl)[4]) {
     int k = 0, s = (int)n;
-    while (s > 10) {
+    while (s > 9) {
         m[k] = 4;
         sl[k] = s - 4;
         s -= 4;

@@ -29,7 +29,7 @@ namespace ffg {
 constexpr uint32_t kPrimeC[3] = {2113929217u, 2013265921u, 1811939329u};
 constexpr uint32_t kLineThreads = 256; // every line kernel runs 256 threads
 constexpr uint32_t kLineThreadsLg = 8;
-constexpr int kLineMinBlocks = 2;     // 128 registers a thread: a 32-point DFT stays in registers
+constexpr int kLineMinBlocks = 3;     // 80 registers a thread
 
 // Filled once per process (set_line_consts in ffg_ntt.cu).
 static __constant__ LineConsts c_lines;
@@ -107,11 +107,10 @@ FFG_DEV_INLINE void dft_dit(uint32_t (&x)[1 << M]) {
 // consecutive j: conflict-free with the padding for sl = 0 or sl >= 5), and
 // the block-lines second; a thread loads its group's twiddles once for all
 // the block-lines it handles.
-template <int PI, int M, bool DIF>
+template <int PI, int M, bool DIF, bool TW>
 FFG_DEV_INLINE void line_step(uint32_t *__restrict__ s, uint32_t lines_lg, uint32_t nblk, uint32_t n,
                               uint32_t stride, uint32_t sl, const uint2 *__restrict__ tw) {
     constexpr int R = 1 << M;
-    constexpr bool kHoist = M <= 4; // 2^M - 1 twiddle pairs kept in registers
     const uint32_t np_lg = n - M;
     const uint32_t tp_lg = np_lg < kLineThreadsLg ? np_lg : kLineThreadsLg;
     const uint32_t tp = threadIdx.x & ((1u << tp_lg) - 1), tl = threadIdx.x >> tp_lg;
@@ -122,8 +121,8 @@ FFG_DEV_INLINE void line_step(uint32_t *__restrict__ s, uint32_t lines_lg, uint3
     for (uint32_t pos = tp; pos < (1u << np_lg); pos += 1u << tp_lg) {
         const uint32_t j = pos & (S - 1);
         const uint32_t base = ((pos >> sl) << (M + sl)) + j;
-        uint2 w[kHoist ? R - 1 : 1];
-        if (kHoist && sl) {
+        uint2 w[TW ? R - 1 : 1];
+        if (TW) {
 #pragma unroll
             for (int t = 1; t < R; t++) w[t - 1] = __ldg(&tw[(t - 1) * S + j]);
         }
@@ -134,14 +133,14 @@ FFG_DEV_INLINE void line_step(uint32_t *__restrict__ s, uint32_t lines_lg, uint3
             for (int t = 0; t < R; t++) x[t] = L[t * Sp];
             if (DIF) {
                 dft_dif<PI, M>(x);
-                if (sl) {
+                if (TW) {
 #pragma unroll
-                    for (int t = 1; t < R; t++) x[t] = sh<PI>(x[t], kHoist ? w[t - 1] : __ldg(&tw[(t - 1) * S + j]));
+                    for (int t = 1; t < R; t++) x[t] = sh<PI>(x[t], w[t - 1]);
                 }
             } else {
-                if (sl) {
+                if (TW) {
 #pragma unroll
-                    for (int t = 1; t < R; t++) x[t] = sh<PI>(x[t], kHoist ? w[t - 1] : __ldg(&tw[(t - 1) * S + j]));
+                    for (int t = 1; t < R; t++) x[t] = sh<PI>(x[t], w[t - 1]);
                 }
                 dft_dit<PI, M>(x);
             }
@@ -151,16 +150,28 @@ FFG_DEV_INLINE void line_step(uint32_t *__restrict__ s, uint32_t lines_lg, uint3
     }
 }
 
+// Steps at stride 1 need no twiddles (j = 0); schedule() gives radix 32
+// only there, so the twiddled steps hold at most 16 words and 15 twiddles.
+// A stride-1 step has the radix of the whole block when n < 6 (the column
+// lines of L = 3 2^11 have n = 3).
 template <int PI, bool DIF>
 FFG_DEV_INLINE void line_step_m(int M, uint32_t *s, uint32_t lines_lg, uint32_t nblk, uint32_t n, uint32_t stride,
                                 uint32_t sl, const uint2 *tw) {
+    if (sl == 0) {
+        switch (M) {
+        case 1: line_step<PI, 1, DIF, false>(s, lines_lg, nblk, n, stride, 0, tw); break;
+        case 2: line_step<PI, 2, DIF, false>(s, lines_lg, nblk, n, stride, 0, tw); break;
+        case 3: line_step<PI, 3, DIF, false>(s, lines_lg, nblk, n, stride, 0, tw); break;
+        case 4: line_step<PI, 4, DIF, false>(s, lines_lg, nblk, n, stride, 0, tw); break;
+        default: line_step<PI, 5, DIF, false>(s, lines_lg, nblk, n, stride, 0, tw); break;
+        }
+        return;
+    }
     switch (M) {
-    case 1: line_step<PI, 1, DIF>(s, lines_lg, nblk, n, stride, sl, tw); break;
-    case 2: line_step<PI, 2, DIF>(s, lines_lg, nblk, n, stride, sl, tw); break;
-    case 3: line_step<PI, 3, DIF>(s, lines_lg, nblk, n, stride, sl, tw); break;
-    case 4: line_step<PI, 4, DIF>(s, lines_lg, nblk, n, stride, sl, tw); break;
-    case 5: line_step<PI, 5, DIF>(s, lines_lg, nblk, n, stride, sl, tw); break;
-    default: break;
+    case 1: line_step<PI, 1, DIF, true>(s, lines_lg, nblk, n, stride, sl, tw); break;
+    case 2: line_step<PI, 2, DIF, true>(s, lines_lg, nblk, n, stride, sl, tw); break;
+    case 3: line_step<PI, 3, DIF, true>(s, lines_lg, nblk, n, stride, sl, tw); break;
+    default: line_step<PI, 4, DIF, true>(s, lines_lg, nblk, n, stride, sl, tw); break;
     }
 }
 
