@@ -8,7 +8,9 @@ One step = one F(n) by fast doubling through the public API (fibonacci()).
 `value` is the device time of the chain (CUDA events on the library's stream,
 operands resident in HBM from the first doubling step on), `e2e` the same
 call timed on the host including the prefix, the copy of the starting pair
-to the device and the copy of F(n) back.  L2 is flushed (a 256 MiB write)
+to the device and the copy of F(n) back.  The roofline figures come from a
+second pass of the same steps with CUDA events around every launch of the
+dominant kernel family (kept out of the timed pass, which they perturb).  L2 is flushed (a 256 MiB write)
 before every step.  With N > 1 every rank computes its own F(n) (replicas:
 the chain is sequential and has no data-parallel split); value is the job's
 ms per F(n), the max over ranks divided by N.  Prints one JSON line on rank 0.
@@ -218,6 +220,85 @@ def run_ntt_microbench(args):
     return 0 if ok else 1
 
 
+def run_uneven(count=4096, reps=3, seed=4):
+    """The uneven product stream: `count` independent products, operand bit
+    lengths log-uniform over 2^10..2^24, aspect up to 16:1, uniform random
+    limbs (seeded), operands resident on the device.  Device ms of
+      plain_unbatched: one call per product, the reference's thresholds;
+      plain: one batched call, the same thresholds;
+      learned: one batched call, the trained cost model choosing per product;
+    each the mean of `reps` runs after a warm-up, L2 flushed before each.
+    e2e: the learned batch through the host API (operands copied in, products
+    copied out).  Every product of the learned run is checked modulo three
+    64-bit primes."""
+    import numpy as np
+    import torch
+    import fastfib_b200 as ff
+    from fastfib_b200.workload import uneven_products
+    ff.init(1 << 22)
+    pairs = uneven_products(seed=seed, count=count)
+    dev = torch.device("cuda")
+    flat_a = torch.from_numpy(np.concatenate([a for a, _ in pairs]).view(np.int64)).to(dev)
+    flat_b = torch.from_numpy(np.concatenate([b for _, b in pairs]).view(np.int64)).to(dev)
+    out_len = sum(a.size + b.size + 1 for a, b in pairs)
+    out = torch.empty(out_len, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    jobs, oa, ob, oo, offs = [], 0, 0, 0, []
+    for a, b in pairs:
+        jobs.append({"a": flat_a.data_ptr() + 8 * oa, "b": flat_b.data_ptr() + 8 * ob, "na": a.size, "nb": b.size,
+                     "bits_a": 64 * a.size, "bits_b": 64 * b.size, "out": out.data_ptr() + 8 * oo})
+        offs.append(oo)
+        oa, ob, oo = oa + a.size, ob + b.size, oo + a.size + b.size + 1
+
+    def timed(fn):
+        ts = []
+        for r in range(reps + 1):
+            flush.fill_(r & 0xFF)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            if r:
+                ts.append(e0.elapsed_time(e1))
+        return statistics.mean(ts)
+
+    stream = torch.cuda.current_stream().cuda_stream
+    res = {}
+    for m in ("plain", "learned"):
+        js = [dict(j, method=m) for j in jobs]
+        res[m] = timed(lambda: ff.mul_batch_device(js, stream))
+    js = [dict(j, method="plain") for j in jobs]
+    res["plain_unbatched"] = timed(lambda: [ff.mul_batch_device([j], stream) for j in js])
+    # correctness of the learned run (the last one executed above was plain
+    # unbatched; run learned once more and check every product)
+    ff.mul_batch_device([dict(j, method="learned") for j in jobs], stream)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().view(np.uint64)
+    with open(GOLD_FP) as f:
+        primes = [int(p) for p in json.load(f)["primes"]][:3]
+    ok = True
+    for (a, b), o in zip(pairs, offs):
+        x, y = int.from_bytes(a.tobytes(), "little"), int.from_bytes(b.tobytes(), "little")
+        z = int.from_bytes(got[o:o + a.size + b.size + 1].tobytes(), "little")
+        if any(z % p != (x % p) * (y % p) % p for p in primes) or z.bit_length() > 64 * (a.size + b.size):
+            ok = False
+            break
+    # end to end through the host API (pinned staging inside the library)
+    ff.mul_batch(pairs[:8], "learned")
+    t = time.perf_counter()
+    ff.mul_batch(pairs, "learned")
+    e2e = (time.perf_counter() - t) * 1e3
+    in_bytes = 8 * (int(flat_a.numel()) + int(flat_b.numel()))
+    return {"workload": f"{count} products, operands log-uniform 2^10..2^24 bits, aspect <= 16, seed {seed}",
+            "plain_unbatched_ms": res["plain_unbatched"], "plain_ms": res["plain"], "learned_ms": res["learned"],
+            "learned_vs_plain": res["plain"] / res["learned"],
+            "batched_learned_vs_plain_unbatched": res["plain_unbatched"] / res["learned"],
+            "e2e_ms": e2e, "h2d_bytes": in_bytes, "d2h_bytes": 8 * out_len, "bit_exact": ok,
+            "l2": "flushed before every timed run"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -227,8 +308,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-f1e9", action="store_true", help="skip the extra F(10^9) measurement")
-    ap.add_argument("--config", default="fib", choices=["fib", "ntt"],
-                    help="fib: F(n) (the headline); ntt: one NTT product of --limbs limbs")
+    ap.add_argument("--config", default="fib", choices=["fib", "ntt", "uneven"],
+                    help="fib: F(n) (the headline); ntt: one NTT product of --limbs limbs; "
+                         "uneven: the uneven product stream, plain against learned dispatch")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-stream figures in the fib line")
     ap.add_argument("--limbs", type=int, default=1 << 22)
     ap.add_argument("--square", action="store_true")
     args = ap.parse_args()
@@ -241,6 +324,12 @@ def main():
         return run_reference(args, rank, world)
     if args.config == "ntt":
         return run_ntt_microbench(args)
+    if args.config == "uneven":
+        r = run_uneven(reps=args.steps)
+        print(json.dumps({"metric": "uneven product stream ms (4096 products), learned vs plain dispatch",
+                          "value": r["learned_ms"], "unit": "ms", "higher_is_better": False, "steps": args.steps,
+                          "dtype": "u32", "config": r}), flush=True)
+        return 0 if r["bit_exact"] else 1
 
     import torch
     import torch.distributed as dist
@@ -266,10 +355,9 @@ def main():
     ok = fingerprint_ok(args.n, r)
     if ok is False:
         raise SystemExit(f"F({args.n}) does not match its golden fingerprint")
-    ff.profile([dominant])
+    ff.profile(False)
     for i in range(max(args.warmup - 1, 2)):
         r = ff.fibonacci(args.n)
-    ff.profile([dominant])  # reset the totals: only the timed steps count
     dev_ms, e2e_ms = [], []
     launches0 = ff.launch_count()
     torch.cuda.synchronize()
@@ -285,9 +373,20 @@ def main():
         torch.cuda.synchronize()
         barrier()
     launches = ff.launch_count() - launches0
+    h2d, d2h = ff.last_chain_io()
+    # the roofline pass: the same K steps again with CUDA events around every
+    # launch of the dominant family (events perturb the chain, so `value`
+    # comes from the pass above, which has none)
+    ff.profile([dominant])
+    for i in range(2):
+        ff.fibonacci(args.n)
+    ff.profile([dominant])  # reset the totals: only these K steps count
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        torch.cuda.synchronize()
+        ff.fibonacci(args.n)
     prof = ff.profile_read()[dominant]
     ff.profile(False)
-    h2d, d2h = ff.last_chain_io()
 
     total_dev = sum(dev_ms)
     total_e2e = sum(e2e_ms)
@@ -330,6 +429,8 @@ def main():
             "clocks": clk.summary(),
             "f1e9": extra or None,
         }
+        if not args.no_uneven and world == 1:
+            line["uneven"] = run_uneven(reps=3)
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.n)
         print(json.dumps(line), flush=True)

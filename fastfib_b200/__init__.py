@@ -22,6 +22,7 @@ import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libfastfib_b200.so")
+TUNING_PATH = os.path.join(PKG, "tuning.txt")  # written by python -m fastfib_b200.tune
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _szp = ctypes.POINTER(ctypes.c_size_t)
@@ -52,7 +53,11 @@ class Job(ctypes.Structure):
 
 
 # methods of a batched product (FFG_M_*)
-METHODS = {"plain": -1, "school": 0, "ntt": 1, "ntt_pow2": 2, "ntt_r3": 3}
+METHODS = {"plain": -1, "school": 0, "ntt": 1, "ntt_pow2": 2, "ntt_r3": 3, "learned": 4}
+# cost-model outputs, in order (FFG_M_SCHOOL .. FFG_M_NTT_R3)
+MODEL_METHODS = ("school", "ntt", "ntt_pow2", "ntt_r3")
+MLP_D, MLP_H, MLP_K = 8, 32, 4
+MLP_NPARAM = MLP_H * MLP_D + MLP_H + MLP_H * MLP_H + MLP_H + MLP_K * MLP_H + MLP_K
 
 
 class FfgError(RuntimeError):
@@ -92,6 +97,18 @@ def lib() -> ctypes.CDLL:
     L.ffg_last_error.restype = ctypes.c_char_p
     L.ffg_free.argtypes = [ctypes.c_void_p]
     L.ffg_mul_batch_host.argtypes = [ctypes.POINTER(Job), ctypes.c_size_t]
+    _fp = ctypes.POINTER(ctypes.c_float)
+    _ip = ctypes.POINTER(ctypes.c_int32)
+    L.ffg_mlp_features.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _fp]
+    L.ffg_mlp_train.argtypes = [_fp, _fp, _ip, _fp, ctypes.c_size_t, ctypes.c_int, ctypes.c_float, _fp]
+    L.ffg_mlp_grad.argtypes = [_fp, _fp, _ip, _fp, ctypes.c_size_t, _fp, _fp]
+    L.ffg_mlp_predict.argtypes = [_fp, _fp, ctypes.c_size_t, _fp]
+    L.ffg_mlp_set.argtypes = [_fp]
+    L.ffg_time_batch.argtypes = [ctypes.POINTER(Job), ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.ffg_set_geometry.argtypes = [ctypes.c_uint32] * 4
+    L.ffg_get_geometry.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+                                   ctypes.POINTER(ctypes.c_uint32)]
+    L.ffg_load_tuning.argtypes = [ctypes.c_char_p]
     L.ffg_mul_batch_device.argtypes = [ctypes.POINTER(Job), ctypes.c_size_t, ctypes.c_void_p]
     L.ffg_release.argtypes = [ctypes.c_void_p]
     for name in ("big_mul", "big_mul_ntt", "big_mul_toom3"):
@@ -107,6 +124,9 @@ def lib() -> ctypes.CDLL:
     L.ntt_init.argtypes = [ctypes.c_size_t]
     L.plat_seconds.restype = ctypes.c_double
     _lib = L
+    # the autotuner's geometry table and cost model, measured on a B200
+    if os.path.exists(TUNING_PATH) and not os.environ.get("FASTFIB_B200_NO_TUNING"):
+        _check(L.ffg_load_tuning(TUNING_PATH.encode()))
     return L
 
 
@@ -213,6 +233,11 @@ def init(max_limbs: int) -> None:
     _check(lib().ffg_init(max_limbs))
 
 
+def ntt_max_L() -> int:
+    """The GPU layer's transform cap (ffg_ntt_max_L)."""
+    return lib().ffg_ntt_max_L()
+
+
 def plan(bits_a: int, bits_b: int, square: bool = False) -> dict:
     p = Plan()
     _check(lib().ffg_plan_select(bits_a, bits_b, int(square), ctypes.byref(p)))
@@ -257,6 +282,10 @@ def mul_batch(pairs, method="ntt") -> list:
 def mul_batch_device(jobs, stream: int = 0) -> None:
     """ffg_mul_batch_device on a list of dicts with device pointers:
     a, b, na, nb, bits_a, bits_b, out (na + nb + 1 limbs), square, method."""
+    _check(lib().ffg_mul_batch_device(_device_jobs(jobs), len(jobs), stream or None))
+
+
+def _device_jobs(jobs):
     arr = (Job * max(1, len(jobs)))()
     for i, d in enumerate(jobs):
         j = arr[i]
@@ -267,7 +296,111 @@ def mul_batch_device(jobs, stream: int = 0) -> None:
         j.out = ctypes.cast(d["out"], _u64p)
         j.square = int(d.get("square", False))
         j.method = METHODS[d.get("method", "ntt")]
-    _check(lib().ffg_mul_batch_device(arr, len(jobs), stream or None))
+    return arr
+
+
+def time_batch(jobs, reps: int = 3) -> float:
+    """ffg_time_batch: device milliseconds of one mul_batch_device call on
+    `jobs` (dicts as mul_batch_device takes), the mean of reps runs."""
+    ms = ctypes.c_double()
+    _check(lib().ffg_time_batch(_device_jobs(jobs), len(jobs), reps, ctypes.byref(ms)))
+    return ms.value
+
+
+# ------------------------------------------------------------ the cost model
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def mlp_features(bits_a: int, bits_b: int, square: bool = False) -> np.ndarray:
+    f = np.zeros(MLP_D, dtype=np.float32)
+    _check(lib().ffg_mlp_features(bits_a, bits_b, int(square), _fptr(f)))
+    return f
+
+
+def mlp_init(seed: int = 0) -> np.ndarray:
+    """Initial parameters: uniform +-sqrt(6 / (fan_in + fan_out)) weights, zero biases."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for fan_in, fan_out in ((MLP_D, MLP_H), (MLP_H, MLP_H), (MLP_H, MLP_K)):
+        lim = np.sqrt(6.0 / (fan_in + fan_out))
+        parts += [rng.uniform(-lim, lim, fan_in * fan_out), np.zeros(fan_out)]
+    return _f32(np.concatenate(parts))
+
+
+def mlp_train(params, X, method, y, epochs: int = 1000, lr: float = 1e-2):
+    """ffg_mlp_train: (trained parameters, loss before each epoch)."""
+    p = _f32(params).copy()
+    X, y = _f32(X), _f32(y)
+    m = np.ascontiguousarray(method, dtype=np.int32)
+    hist = np.zeros(max(1, epochs), dtype=np.float32)
+    _check(lib().ffg_mlp_train(_fptr(p), _fptr(X), m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _fptr(y),
+                               len(y), epochs, lr, _fptr(hist)))
+    return p, hist[:epochs]
+
+
+def mlp_grad(params, X, method, y):
+    """ffg_mlp_grad: (loss, gradient) from the GPU kernel."""
+    p, X, y = _f32(params), _f32(X), _f32(y)
+    m = np.ascontiguousarray(method, dtype=np.int32)
+    g = np.zeros(MLP_NPARAM, dtype=np.float32)
+    loss = ctypes.c_float()
+    _check(lib().ffg_mlp_grad(_fptr(p), _fptr(X), m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _fptr(y),
+                              len(y), _fptr(g), ctypes.byref(loss)))
+    return loss.value, g
+
+
+def mlp_predict(params, X) -> np.ndarray:
+    """ffg_mlp_predict: every output for the rows of X (params None: the installed model)."""
+    X = _f32(X)
+    out = np.zeros((X.shape[0], MLP_K), dtype=np.float32)
+    p = None if params is None else _f32(params)
+    _check(lib().ffg_mlp_predict(None if p is None else _fptr(p), _fptr(X), X.shape[0], _fptr(out)))
+    return out
+
+
+def set_model(params) -> None:
+    """ffg_mlp_set: installs the cost model for method "learned" (None removes it)."""
+    p = None if params is None else _f32(params)
+    _check(lib().ffg_mlp_set(None if p is None else _fptr(p)))
+
+
+def load_tuning(path: str = TUNING_PATH) -> bool:
+    """ffg_load_tuning: installs the autotuner's geometry table and cost
+    model; False if the file does not exist."""
+    if not os.path.exists(path):
+        return False
+    _check(lib().ffg_load_tuning(path.encode()))
+    return True
+
+
+def set_geometry(lg: int, r3: int, row_lg: int, wc: int) -> None:
+    _check(lib().ffg_set_geometry(lg, r3, row_lg, wc))
+
+
+def get_geometry(lg: int, r3: int) -> tuple:
+    c, w = ctypes.c_uint32(), ctypes.c_uint32()
+    _check(lib().ffg_get_geometry(lg, r3, ctypes.byref(c), ctypes.byref(w)))
+    return c.value, w.value
+
+
+def write_tuning(path: str, geometry, params, comment: str = "") -> None:
+    """The tuning file ffg_load_tuning reads: geometry rows (lg, r3, row_lg,
+    wc) and the cost model's parameters."""
+    with open(path, "w") as f:
+        f.write("# fastfib_b200 tuning: four-step geometry and cost model\n")
+        for line in comment.splitlines():
+            f.write(f"# {line}\n")
+        for lg, r3, c, wc in geometry:
+            f.write(f"geometry {lg} {r3} {c} {wc}\n")
+        if params is not None:
+            p = _f32(params)
+            f.write(f"mlp {p.size} " + " ".join(f"{v:.9g}" for v in p) + "\n")
 
 
 def mul_device(out_ptr: int, a_ptr: int, na: int, bits_a: int, b_ptr: int, nb: int, bits_b: int,

@@ -10,8 +10,8 @@
 //      overlap it (3-6 of them): the column sum lo_j + 2^64 hi_j.  This is the
 //      reference's crt_pack64 (src/crt.c:70-87) with the running carry turned
 //      into per-limb sums.
-//   3. cta_resolve (ffg_ripple.cuh) settles the one-bit ripples; k_settle
-//      carries between CTAs.
+//   3. cta_resolve (ffg_ripple.cuh) settles the one-bit ripples; the CTA
+//      that finishes last settles the carries between CTAs (settle_cta).
 // A small signed constant is added to the product on the way (the final
 // +-2 of fast doubling, src/fib.c:249) in two's complement over the output.
 //
@@ -40,6 +40,9 @@ FFG_DEV_INLINE uint32_t crt_ctas_dev(uint64_t nlimbs, uint32_t width) {
 }
 
 FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t cta);
+FFG_DEV_INLINE void settle_cta(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *maps,
+                               uint32_t ncta);
+FFG_DEV_INLINE bool last_cta(uint32_t *ticket, uint32_t ncta);
 
 __global__ void __launch_bounds__(CRT_THREADS) k_crt(GarnerConst K, CrtJob J) { crt_block(K, J, blockIdx.x); }
 
@@ -139,30 +142,34 @@ FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t ct
     const uint32_t map = cta_resolve(lo, hi, cta ? hiprev_s : 0, NL, gG, gP, gin);
     for (uint32_t j = threadIdx.x; j < NL && j0 + j < J.nlimbs; j += blockDim.x) J.out[j0 + j] = lo[j];
     if (threadIdx.x == 0) J.maps[cta] = map;
+    const uint32_t ncta = crt_ctas_dev(J.nlimbs, b);
+    if (ncta > 1 && last_cta(J.ticket, ncta)) {
+        settle_cta(J.out, J.nlimbs, NL, J.maps, ncta);
+        if (threadIdx.x == 0) *J.ticket = 0;
+    }
 }
 
-// Carries between CTAs: one block of SETTLE_THREADS threads per product.
-// Thread t composes the maps of its run of consecutive CTAs, a block-wide
-// scan of those composites gives the carry into every run (carry 0 into the
-// first CTA), and each thread walks its run again adding the carry into the
-// CTAs that receive one (a carry stops at the first limb that does not wrap).
-constexpr uint32_t SETTLE_THREADS = 1024;
-
-FFG_DEV_INLINE void settle_block(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *__restrict__ maps,
-                                 uint32_t ncta) {
-    __shared__ uint32_t wpre[SETTLE_THREADS / 32];
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t per = (ncta + SETTLE_THREADS - 1) / SETTLE_THREADS;
+// Carries between CTAs, settled by the CTA that finishes last (all of its
+// threads): thread t composes the maps of its run of consecutive CTAs, a
+// block-wide scan of those composites gives the carry into every run (carry
+// 0 into the first CTA), and each thread walks its run again adding the
+// carry into the CTAs that receive one (a carry stops at the first limb that
+// does not wrap).  Maps and limbs written by other CTAs are read through L2.
+FFG_DEV_INLINE void settle_cta(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *maps,
+                               uint32_t ncta) {
+    __shared__ uint32_t wpre[32];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t per = (ncta + blockDim.x - 1) / blockDim.x;
     const uint32_t q0 = min(ncta, threadIdx.x * per), q1 = min(ncta, q0 + per);
     uint32_t run = 2u; // identity: c -> c
-    for (uint32_t q = q0; q < q1; q++) run = map_then(run, maps[q]);
+    for (uint32_t q = q0; q < q1; q++) run = map_then(run, __ldcg(&maps[q]));
     const uint32_t inc = warp_map_scan(run);
     if (lane == 31) wpre[warp] = inc;
     __syncthreads();
     if (warp == 0) {
-        const uint32_t v = warp_map_scan(wpre[lane]); // SETTLE_THREADS / 32 == 32 warps
+        const uint32_t v = warp_map_scan(lane < nw ? wpre[lane] : 2u);
         __syncwarp();
-        wpre[lane] = v;
+        if (lane < nw) wpre[lane] = v;
     }
     __syncthreads();
     uint32_t exc = __shfl_up_sync(0xffffffffu, inc, 1);
@@ -172,31 +179,27 @@ FFG_DEV_INLINE void settle_block(uint64_t *out, uint64_t nlimbs, uint32_t cta_li
     for (uint32_t q = q0; q < q1; q++) {
         if (carry) {
             const uint64_t end = min(nlimbs, (uint64_t)(q + 1) * cta_limbs);
-            for (uint64_t j = (uint64_t)q * cta_limbs; j < end; j++)
-                if (++out[j] != 0) break;
+            for (uint64_t j = (uint64_t)q * cta_limbs; j < end; j++) {
+                const uint64_t v = __ldcg(&out[j]) + 1;
+                out[j] = v;
+                if (v != 0) break;
+            }
         }
-        carry = map_apply(maps[q], carry);
+        carry = map_apply(__ldcg(&maps[q]), carry);
     }
+    __syncthreads();
 }
 
-__global__ void __launch_bounds__(SETTLE_THREADS) k_settle(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs,
-                                                           const uint32_t *__restrict__ maps, uint32_t ncta) {
-    settle_block(out, nlimbs, cta_limbs, maps, ncta);
-}
-
-// Settles a batch of CRTs (blockIdx.y the product).
-__global__ void __launch_bounds__(SETTLE_THREADS) k_settle_crt_batch(const CrtJob *__restrict__ jobs) {
-    const CrtJob J = jobs[blockIdx.y];
-    const uint32_t ncta = crt_ctas_dev(J.nlimbs, J.width);
-    if (ncta <= 1) return;
-    settle_block(J.out, J.nlimbs, CRT_NL_PER_W * J.width, J.maps, ncta);
-}
-
-static cudaError_t launch_settle(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *maps,
-                                 uint32_t ncta, cudaStream_t st) {
-    if (ncta <= 1) return cudaSuccess; // nothing comes into the first CTA
-    k_settle<<<1, SETTLE_THREADS, 0, st>>>(out, nlimbs, cta_limbs, maps, ncta);
-    return cudaGetLastError();
+// Called by every CTA of a launch after its limbs and map are written:
+// true in the one CTA that takes the last of ncta tickets.
+FFG_DEV_INLINE bool last_cta(uint32_t *ticket, uint32_t ncta) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == ncta - 1;
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
 }
 
 uint32_t crt_ctas(uint64_t nlimbs, uint32_t width) {
@@ -220,12 +223,7 @@ cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st) {
     prof_begin(PK_CRT, st);
     k_crt<<<ncta, CRT_THREADS, crt_smem(), st>>>(garner_const(), J);
     prof_end(PK_CRT, st, 12.0 * (double)J.conv + 8.0 * (double)J.nlimbs);
-    cudaError_t e = cudaGetLastError();
-    if (e) return e;
-    prof_begin(PK_CARRY, st);
-    e = launch_settle(J.out, J.nlimbs, CRT_NL_PER_W * J.width, J.maps, ncta, st);
-    prof_end(PK_CARRY, st, 4.0 * ncta);
-    return e;
+    return cudaGetLastError();
 }
 
 cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
@@ -241,11 +239,6 @@ cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_
     prof_begin(PK_CRT, st);
     k_crt_batch<<<dim3(max_ctas, count), CRT_THREADS, crt_smem(), st>>>(garner_const(), d_jobs);
     prof_end(PK_CRT, st, bytes);
-    cudaError_t e = cudaGetLastError();
-    if (e || max_ctas <= 1) return e;
-    prof_begin(PK_CARRY, st);
-    k_settle_crt_batch<<<dim3(1, count), SETTLE_THREADS, 0, st>>>(d_jobs);
-    prof_end(PK_CARRY, st, 4.0 * max_ctas * count);
     return cudaGetLastError();
 }
 
@@ -255,7 +248,7 @@ cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_
 // threads per CTA and SCHOOL_NL output limbs (columns) per CTA.  Column j
 // sums a_i b_(j-i) over the shorter operand into 192 bits (t0, t1, t2); then
 // v_j = t0_j + t1_(j-1) + t2_(j-2) < 3 2^64 leaves single-bit ripples for
-// cta_resolve, and carries between CTAs go through k_settle_school.
+// cta_resolve, and the last CTA settles the carries between CTAs.
 constexpr uint32_t SCHOOL_NL = 1024;
 constexpr uint32_t SCHOOL_THREADS = 256;
 
@@ -313,13 +306,11 @@ __global__ void __launch_bounds__(SCHOOL_THREADS) k_school(const SchoolJob *__re
     const uint32_t map = cta_resolve(lo, hi, blockIdx.x ? hiprev_s : 0, SCHOOL_NL, gG, gP, gin);
     for (uint32_t j = threadIdx.x; j < SCHOOL_NL && (uint64_t)j0 + j < J.nlimbs; j += blockDim.x) J.out[j0 + j] = lo[j];
     if (threadIdx.x == 0) J.maps[blockIdx.x] = map;
-}
-
-__global__ void __launch_bounds__(SETTLE_THREADS) k_settle_school_batch(const SchoolJob *__restrict__ jobs) {
-    const SchoolJob J = jobs[blockIdx.y];
     const uint32_t ncta = school_ctas(J.nlimbs);
-    if (ncta <= 1) return;
-    settle_block(J.out, J.nlimbs, SCHOOL_NL, J.maps, ncta);
+    if (ncta > 1 && last_cta(J.ticket, ncta)) {
+        settle_cta(J.out, J.nlimbs, SCHOOL_NL, J.maps, ncta);
+        if (threadIdx.x == 0) *J.ticket = 0;
+    }
 }
 
 cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
@@ -328,11 +319,6 @@ cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_
     prof_begin(PK_SCHOOL, st);
     k_school<<<dim3(max_ctas, count), SCHOOL_THREADS, 0, st>>>(d_jobs);
     prof_end(PK_SCHOOL, st, bytes);
-    cudaError_t e = cudaGetLastError();
-    if (e || max_ctas <= 1) return e;
-    prof_begin(PK_CARRY, st);
-    k_settle_school_batch<<<dim3(1, count), SETTLE_THREADS, 0, st>>>(d_jobs);
-    prof_end(PK_CARRY, st, 4.0 * max_ctas * count);
     return cudaGetLastError();
 }
 
@@ -405,6 +391,10 @@ __global__ void __launch_bounds__(LIN_THREADS) k_lin(LinJob J) {
         if (threadIdx.x == 0) J.maps[(size_t)k * gridDim.x + blockIdx.x] = map;
         __syncthreads();
     }
+    if (gridDim.x > 1 && last_cta(J.ticket, gridDim.x)) {
+        for (uint32_t k = 0; k < J.nout; k++) settle_cta(k ? J.out[1] : J.out[0], J.len, LIN_NL, J.maps + (size_t)k * gridDim.x, gridDim.x);
+        if (threadIdx.x == 0) *J.ticket = 0;
+    }
 }
 
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st) {
@@ -412,13 +402,7 @@ cudaError_t launch_lin(const LinJob &J, cudaStream_t st) {
     prof_begin(PK_LIN, st);
     k_lin<<<ncta, LIN_THREADS, 0, st>>>(J);
     prof_end(PK_LIN, st, 8.0 * (double)(J.n1 + J.n2) + 8.0 * (double)J.len * J.nout);
-    cudaError_t e = cudaGetLastError();
-    if (e) return e;
-    prof_begin(PK_CARRY, st);
-    for (uint32_t k = 0; k < J.nout && !e; k++)
-        e = launch_settle(J.out[k], J.len, LIN_NL, J.maps + (size_t)k * ncta, ncta, st);
-    prof_end(PK_CARRY, st, 4.0 * ncta * J.nout);
-    return e;
+    return cudaGetLastError();
 }
 
 } // namespace ffg

@@ -76,6 +76,25 @@ struct Ctx {
 static Ctx g;
 static std::recursive_mutex g_mu;
 
+// ------------------------------------------------------------ ticket pool
+
+// Zero words for the in-launch carry settle (see ticket_get in
+// ffg_internal.h): the live region is handed out round-robin, captured
+// launches take words of the capture region (a cached graph keeps its words
+// while later work cycles through the live region), and the last word
+// belongs to the allocation-free multiply.
+constexpr uint32_t kTicketsLive = 1u << 16, kTicketsCapture = 1u << 13;
+static uint32_t *g_tickets = nullptr;
+static uint32_t g_ticket_live = 0, g_ticket_cap = 0;
+static bool g_capturing = false, g_capture_starved = false;
+
+uint32_t *ticket_get() {
+    if (g_capturing) return g_tickets + kTicketsLive + (g_ticket_cap++ % kTicketsCapture);
+    return g_tickets + (g_ticket_live++ % kTicketsLive);
+}
+
+static uint32_t *ticket_get_reserved() { return g_tickets + kTicketsLive + kTicketsCapture; }
+
 // ------------------------------------------------------------ profiling
 
 // Launch counter (always on) and, when enabled, CUDA-event brackets around
@@ -103,8 +122,6 @@ static cudaEvent_t ev_get() {
     cudaEventCreate(&e);
     return e;
 }
-
-static bool g_capturing = false, g_capture_starved = false;
 
 // Inside a stream capture an event becomes a timing node of the graph only
 // when recorded as external.
@@ -196,6 +213,11 @@ static int build_tables() {
     const size_t per = nstw * 2 * sizeof(uint2) + nr3 * 2 * sizeof(uint4) + (FFG_TW_LO + ntwh) * sizeof(uint32_t);
     std::vector<char> host(per * 3);
     CK(cudaMalloc(&g.tables, per * 3));
+    if (!g_tickets) {
+        const size_t nt = (size_t)kTicketsLive + kTicketsCapture + 1;
+        CK(cudaMalloc(&g_tickets, nt * sizeof(uint32_t)));
+        CK(cudaMemset(g_tickets, 0, nt * sizeof(uint32_t)));
+    }
     for (int k = 0; k < 3; k++) {
         const uint32_t p = kP[k], gen = kG[k];
         char *hb = host.data() + per * k;
@@ -365,10 +387,34 @@ static uint64_t ntt_length(uint64_t conv, uint32_t *lg_out, uint32_t *r3_out) {
     return L;
 }
 
+// Tuned four-step geometry per transform length 2^lg / 3 2^lg
+// (ffg_set_geometry, from the autotuner): row length 2^c and column-tile
+// width wc; unset entries follow the default rule below.
+struct Geo {
+    uint8_t set, c, wc;
+};
+static Geo g_geo[32][2];
+
+// Shared memory of a four-step column tile (words) and row pass must fit one
+// CTA; the radix-3 tables cover column lines 3 2^n with n < kR3TabLg.
+static bool geo_valid(uint32_t lg, uint32_t r3, uint32_t c, uint32_t wc) {
+    if (c < 4 || c > 13 || c > lg || wc < 8 || wc > 64 || (wc & (wc - 1)) || wc > (1u << c)) return false;
+    const uint32_t rn = lg - c;
+    if (rn < 2 || rn > (r3 ? (uint32_t)kR3TabLg - 1 : (uint32_t)FFG_LINE_LG)) return false;
+    const uint32_t R = (r3 ? 3u : 1u) << rn;
+    return (size_t)line_stride(R) * wc * 4 <= 200 * 1024;
+}
+
 static void gpu_geometry(ffg_plan *pl) {
     if (pl->L <= kSmallMaxL && !pl->split) {
         pl->kernel = 0;
         pl->row_lg = 0;
+        return;
+    }
+    const Geo &t = g_geo[pl->lg & 31][pl->r3 ? 1 : 0];
+    if (t.set && geo_valid(pl->lg, pl->r3, t.c, t.wc)) {
+        pl->kernel = 1;
+        pl->row_lg = t.c;
         return;
     }
     int c = (int)pl->lg - 7;
@@ -459,6 +505,8 @@ static FourStep four_step_geometry(const ffg_plan &pl, bool square) {
     wc = wc < 8 ? 8 : (wc > 64 ? 64 : wc);
     while (wc & (wc - 1)) wc &= wc - 1;
     if (wc > (1u << G.c)) wc = 1u << G.c;
+    const Geo &t = g_geo[pl.lg & 31][pl.r3 ? 1 : 0];
+    if (t.set && t.c == G.c && geo_valid(pl.lg, pl.r3, t.c, t.wc)) wc = t.wc;
     G.wc = wc;
     G.wc_lg = (uint32_t)__builtin_ctz(wc);
     G.col_stride = line_stride(G.R);
@@ -534,6 +582,7 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
         C.add = pr[i].add;
         C.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(C.nlimbs, w) * sizeof(uint32_t));
         if (!C.maps) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
+        C.ticket = ticket_get();
         e = launch_crt(g.P3, C, st);
         if (e) return fail(FFG_E_CUDA, "crt: %s", cudaGetErrorString(e));
     }
@@ -612,6 +661,7 @@ static int run_split(const Prod &pr, bool square, const ffg_plan &pl, cudaStream
     C.add = pr.add;
     C.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(C.nlimbs, w) * sizeof(uint32_t));
     if (!C.maps) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
+    C.ticket = ticket_get();
     e = launch_crt(g.P3, C, st);
     if (e) return fail(FFG_E_CUDA, "crt: %s", cudaGetErrorString(e));
     return FFG_OK;
@@ -663,6 +713,7 @@ static int lin(const uint64_t *s1, uint64_t n1, const uint64_t *s2, uint64_t n2,
     J.alpha[1] = a1, J.beta[1] = b1, J.gamma[1] = g1;
     J.nout = (uint32_t)nout;
     J.maps = (uint32_t *)arena_alloc(2 * (size_t)lin_ctas(len) * sizeof(uint32_t));
+    J.ticket = ticket_get();
     if (!J.maps) return fail(FFG_E_NOMEM, "device arena: linear pass scratch");
     cudaError_t e = launch_lin(J, st);
     if (e) return fail(FFG_E_CUDA, "linear pass: %s", cudaGetErrorString(e));
@@ -768,6 +819,12 @@ struct ChainGraph {
     std::vector<ProfPair> prof;
 };
 static std::vector<ChainGraph> g_chains;
+
+static void chain_cache_clear() {
+    for (auto &c : g_chains)
+        if (c.exec) cudaGraphExecDestroy(c.exec);
+    g_chains.clear();
+}
 
 // Results come back to the host in pinned buffers (a DMA straight into the
 // caller's memory, no staging copy).  They are pooled: ffg_free / ffg_release
@@ -946,7 +1003,20 @@ struct BJob {
     ffg_plan pl;
 };
 
-// The plan a method gives one product (methods: include/ffg.h FFG_M_*).
+// The smallest lengths 2^k >= conv and 3 2^k >= conv (at least 16 and 48),
+// as ntt_length (src/mul_ntt.c:78-93) spans them.
+static void forced_lengths(uint64_t conv, uint64_t *Lp2, uint32_t *lgp2, uint64_t *Lr3, uint32_t *lgr3) {
+    uint64_t L = 16;
+    uint32_t lg = 4;
+    while (L < conv) L <<= 1, lg++;
+    uint64_t L3 = 48;
+    uint32_t lg3 = 4;
+    while (L3 < conv) L3 <<= 1, lg3++;
+    *Lp2 = L, *lgp2 = lg, *Lr3 = L3, *lgr3 = lg3;
+}
+
+// The plan a method gives one product (methods: include/ffg.h FFG_M_*;
+// FFG_M_LEARNED is resolved before this).
 static int method_plan(int method, uint64_t bits_a, uint64_t bits_b, int square, BJob *j) {
     const uint64_t la = (bits_a + 63) / 64, lb = (bits_b + 63) / 64, minlen = la < lb ? la : lb;
     j->school = 0;
@@ -966,20 +1036,109 @@ static int method_plan(int method, uint64_t bits_a, uint64_t bits_b, int square,
     if (method != FFG_M_NTT_POW2 && method != FFG_M_NTT_R3) return fail(FFG_E_ARG, "unknown method %d", method);
     // the same width, the transform length forced to 2^k or 3 2^k
     ffg_plan q = j->pl;
-    const uint64_t conv = q.conv;
-    uint64_t L = 16;
-    uint32_t lg = 4;
-    while (L < conv) L <<= 1, lg++;
-    if (method == FFG_M_NTT_R3) {
-        uint64_t L3 = 48;
-        uint32_t lg3 = 4;
-        while (L3 < conv) L3 <<= 1, lg3++;
-        L = L3, lg = lg3;
-    }
+    uint64_t Lp2, Lr3;
+    uint32_t lgp2, lgr3;
+    forced_lengths(q.conv, &Lp2, &lgp2, &Lr3, &lgr3);
+    const uint64_t L = method == FFG_M_NTT_R3 ? Lr3 : Lp2;
     if (L > g.max_L) return FFG_OK; // past the cap: keep the reference's plan
-    q.L = L, q.lg = lg, q.r3 = method == FFG_M_NTT_R3;
+    q.L = L, q.lg = method == FFG_M_NTT_R3 ? lgr3 : lgp2, q.r3 = method == FFG_M_NTT_R3;
     gpu_geometry(&q);
     j->pl = q;
+    return FFG_OK;
+}
+
+// ------------------------------------------------------------ cost model
+
+static float *g_mlp = nullptr;         // installed parameters on the device (FFG_MLP_NPARAM floats)
+static std::vector<float> g_mlp_host;  // the installed parameters, uploaded on first use
+static bool g_mlp_dirty = false;
+
+// The installed model on the device (nullptr: none); uploads it after ffg_mlp_set.
+static float *mlp_device() {
+    if (g_mlp_host.empty()) return nullptr;
+    if (g_mlp_dirty || !g_mlp) {
+        if (!g_mlp && cudaMalloc(&g_mlp, FFG_MLP_NPARAM * sizeof(float)) != cudaSuccess) {
+            g_mlp = nullptr;
+            return nullptr;
+        }
+        if (cudaMemcpy(g_mlp, g_mlp_host.data(), FFG_MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice)) return nullptr;
+        g_mlp_dirty = false;
+    }
+    return g_mlp;
+}
+static const float kLearnedMargin = 0.152f; // log2(1 / 0.9): a 10% predicted saving
+
+// Features of a product: log2 limbs of the longer and shorter operand,
+// squaring, log2 and radix of the reference plan's length, log2 of the
+// forced 2^k and 3 2^k lengths, and whether the reference plan leaves the
+// one-CTA kernel.  Lengths over 2^26 scale past 1.
+static void mlp_features(uint64_t bits_a, uint64_t bits_b, int square, float *f) {
+    if (square) bits_b = bits_a;
+    const double la = std::log2((double)std::max<uint64_t>(1, (bits_a + 63) / 64));
+    const double lb = std::log2((double)std::max<uint64_t>(1, (bits_b + 63) / 64));
+    ffg_plan pl;
+    plan_select(std::max<uint64_t>(1, bits_a), std::max<uint64_t>(1, bits_b), square, &pl);
+    uint64_t Lp2, Lr3;
+    uint32_t lgp2, lgr3;
+    forced_lengths(pl.conv, &Lp2, &lgp2, &Lr3, &lgr3);
+    f[0] = (float)(std::max(la, lb) / 20.0);
+    f[1] = (float)(std::min(la, lb) / 20.0);
+    f[2] = square ? 1.f : 0.f;
+    f[3] = (float)(std::log2((double)pl.L) / 26.0);
+    f[4] = pl.r3 ? 1.f : 0.f;
+    f[5] = (float)(std::log2((double)Lp2) / 26.0);
+    f[6] = (float)(std::log2((double)Lr3) / 26.0);
+    f[7] = pl.split || pl.L > kSmallMaxL ? 1.f : 0.f;
+}
+
+// Resolves FFG_M_LEARNED in meth[]: one inference launch over every such
+// product, then per product the method of least predicted cost among those
+// whose plan exists (the forced lengths within the cap).  Without a model,
+// and for products the reference splits, the plain thresholds.
+static int learned_resolve(const uint64_t *ba, const uint64_t *bb, const int *sq, int *meth, size_t count,
+                           cudaStream_t st) {
+    std::vector<size_t> idx;
+    for (size_t i = 0; i < count; i++)
+        if (meth[i] == FFG_M_LEARNED) idx.push_back(i);
+    if (idx.empty()) return FFG_OK;
+    float *model = mlp_device();
+    if (!model) {
+        if (!g_mlp_host.empty()) return fail(FFG_E_CUDA, "cost model upload");
+        for (size_t i : idx) meth[i] = FFG_M_PLAIN;
+        return FFG_OK;
+    }
+    std::vector<float> X(idx.size() * FFG_MLP_D), out(idx.size() * FFG_MLP_K);
+    for (size_t k = 0; k < idx.size(); k++) mlp_features(ba[idx[k]], bb[idx[k]], sq[idx[k]], &X[k * FFG_MLP_D]);
+    float *dX = (float *)arena_alloc(X.size() * sizeof(float)), *dO = (float *)arena_alloc(out.size() * sizeof(float));
+    if (!dX || !dO) return fail(FFG_E_NOMEM, "device arena: cost model rows");
+    CK(cudaMemcpyAsync(dX, X.data(), X.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    cudaError_t e = launch_mlp_infer(model, dX, (uint32_t)idx.size(), dO, st);
+    if (e) return fail(FFG_E_CUDA, "cost model inference: %s", cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(out.data(), dO, out.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (size_t k = 0; k < idx.size(); k++) {
+        const size_t i = idx[k];
+        ffg_plan pl;
+        plan_select(std::max<uint64_t>(1, ba[i]), std::max<uint64_t>(1, bb[i]), sq[i], &pl);
+        if (pl.split) {
+            meth[i] = FFG_M_PLAIN;
+            continue;
+        }
+        uint64_t Lp2, Lr3;
+        uint32_t lgp2, lgr3;
+        forced_lengths(pl.conv, &Lp2, &lgp2, &Lr3, &lgr3);
+        // the plain thresholds judge: another method must be predicted at
+        // least kLearnedMargin cheaper (log2 units) than the plain one
+        const uint64_t minlen = std::min((ba[i] + 63) / 64, (bb[i] + 63) / 64);
+        const int plain = minlen >= 200 ? FFG_M_NTT : FFG_M_SCHOOL;
+        const float *o = &out[k * FFG_MLP_K];
+        int best = plain;
+        for (int m = 0; m < FFG_MLP_K; m++) {
+            if ((m == FFG_M_NTT_POW2 && Lp2 > g.max_L) || (m == FFG_M_NTT_R3 && Lr3 > g.max_L)) continue;
+            if (o[m] < o[best] && o[m] < o[plain] - kLearnedMargin) best = m;
+        }
+        meth[i] = best;
+    }
     return FFG_OK;
 }
 
@@ -994,7 +1153,7 @@ struct GroupKey {
 // group of products sharing an NTT plan one transform launch set and one CRT
 // launch; split products one by one.  Job records go to the device in one
 // copy.
-static int run_batch(std::vector<BJob> &jobs, cudaStream_t st) {
+static int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capture = nullptr) {
     std::vector<SchoolJob> sj;
     std::map<GroupKey, std::vector<size_t>> groups;
     std::vector<size_t> splits;
@@ -1010,6 +1169,7 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st) {
             s.nlimbs = J.na + (J.square ? J.na : J.nb) + 1;
             s.maps = (uint32_t *)arena_alloc((size_t)school_ctas(s.nlimbs) * 4);
             if (!s.maps) return fail(FFG_E_NOMEM, "device arena: schoolbook maps");
+            s.ticket = ticket_get();
             school_ctas_max = std::max(school_ctas_max, school_ctas(s.nlimbs));
             school_bytes += 8.0 * (double)(s.na + s.nb + s.nlimbs);
             sj.push_back(s);
@@ -1074,6 +1234,7 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st) {
             r.y = ya, r.y_stride = L, r.conv = ca + cb - 1, r.out = J.out, r.nlimbs = J.na + nb + 1, r.width = w;
             r.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(r.nlimbs, w) * 4);
             if (!r.maps) return fail(FFG_E_NOMEM, "device arena: batch carry maps");
+            r.ticket = ticket_get();
             ln.crt_ctas_max = std::max(ln.crt_ctas_max, crt_ctas(r.nlimbs, w));
             ln.crt_bytes += 12.0 * (double)r.conv + 8.0 * (double)r.nlimbs;
             rj.push_back(r);
@@ -1088,12 +1249,33 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st) {
         if (!dimg) return fail(FFG_E_NOMEM, "device arena: batch job records");
         CK(cudaMemcpyAsync(dimg, img.data(), img.size(), cudaMemcpyHostToDevice, st));
     }
+    // with `capture`, the launches (not the job upload) become a CUDA graph
+    // instead of running: the autotuner replays it to time the device alone
+    if (capture) {
+        if (!splits.empty()) return fail(FFG_E_ARG, "batch capture: split products allocate while running");
+        CK(cudaStreamSynchronize(st));
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        g_capturing = true;
+    }
+    auto end_capture = [&](int rc) -> int {
+        if (!capture) return rc;
+        g_capturing = false;
+        cudaGraph_t gr = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(st, &gr);
+        if (rc) {
+            if (gr) cudaGraphDestroy(gr);
+            return rc;
+        }
+        if (ce) return fail(FFG_E_CUDA, "batch capture: %s", cudaGetErrorString(ce));
+        *capture = gr;
+        return FFG_OK;
+    };
     cudaError_t e;
     for (size_t base = 0; base < sj.size(); base += 65535) {
         const uint32_t cnt = (uint32_t)std::min<size_t>(65535, sj.size() - base);
         e = launch_school_batch((const SchoolJob *)(dimg + school_off) + base, cnt, school_ctas_max, st,
                                 school_bytes * cnt / sj.size());
-        if (e) return fail(FFG_E_CUDA, "schoolbook batch: %s", cudaGetErrorString(e));
+        if (e) return end_capture(fail(FFG_E_CUDA, "schoolbook batch: %s", cudaGetErrorString(e)));
     }
     for (const Launch &ln : launches) {
         const bool sq = ln.key.square != 0;
@@ -1101,7 +1283,7 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st) {
             ConvJobs cjs{};
             cjs.ext = (const ConvJob *)(dimg + ln.conv_off);
             e = launch_conv_small(g.P3, cjs, (uint32_t)ln.count, (uint32_t)ln.pl.L, !sq, st, ln.conv_bytes);
-            if (e) return fail(FFG_E_CUDA, "batched one-CTA transforms: %s", cudaGetErrorString(e));
+            if (e) return end_capture(fail(FFG_E_CUDA, "batched one-CTA transforms: %s", cudaGetErrorString(e)));
         } else {
             FourStep G = four_step_geometry(ln.pl, sq);
             const size_t per = sq ? 65535 : 32767;
@@ -1110,14 +1292,14 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st) {
                 fjs.ext = (const FSJob *)(dimg + ln.conv_off) + base;
                 const uint32_t cnt = (uint32_t)std::min(per, ln.count - base);
                 e = launch_four_step(g.P3, G, fjs, cnt, st, ln.conv_bytes * cnt / ln.count);
-                if (e) return fail(FFG_E_CUDA, "batched four-step: %s", cudaGetErrorString(e));
+                if (e) return end_capture(fail(FFG_E_CUDA, "batched four-step: %s", cudaGetErrorString(e)));
             }
         }
         for (size_t base = 0; base < ln.count; base += 65535) {
             const uint32_t cnt = (uint32_t)std::min<size_t>(65535, ln.count - base);
             e = launch_crt_batch((const CrtJob *)(dimg + ln.crt_off) + base, cnt, ln.crt_ctas_max, st,
                                  ln.crt_bytes * cnt / ln.count);
-            if (e) return fail(FFG_E_CUDA, "batched CRT: %s", cudaGetErrorString(e));
+            if (e) return end_capture(fail(FFG_E_CUDA, "batched CRT: %s", cudaGetErrorString(e)));
         }
     }
     for (size_t idx : splits) {
@@ -1127,7 +1309,7 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st) {
         int rc = run_split(p, J.square != 0, J.pl, st);
         if (rc) return rc;
     }
-    return FFG_OK;
+    return end_capture(FFG_OK);
 }
 
 } // namespace ffg
@@ -1280,10 +1462,15 @@ extern "C" void ffg_shutdown(void) {
     std::lock_guard<std::recursive_mutex> lk(g_mu);
     if (!g.ready) return;
     cudaStreamSynchronize(g.stream);
+    chain_cache_clear();
     for (auto &b : g.blocks) cudaFree(b.ptr);
     g.blocks.clear();
     cudaFree(g.tables);
     g.tables = nullptr;
+    if (g_mlp) cudaFree(g_mlp);
+    g_mlp = nullptr;
+    if (g_tickets) cudaFree(g_tickets);
+    g_tickets = nullptr;
     for (auto &b : g_pinned_pool) cudaFreeHost(b.first);
     g_pinned_pool.clear();
     cudaEventDestroy(g.ev0);
@@ -1397,9 +1584,41 @@ extern "C" int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t n
     C.width = w;
     C.add = 0;
     C.maps = (uint32_t *)(s + o_maps);
+    C.ticket = ticket_get_reserved();
     e = launch_crt(g.P3, C, st);
     if (e) return fail(FFG_E_CUDA, "ffg_mul_device_noalloc crt: %s", cudaGetErrorString(e));
     return FFG_OK;
+}
+
+// One batch of device jobs on stream st (the arena is reset first); with
+// capture, its launches are captured into a graph instead of run.
+static int batch_device_core(ffg_job *jobs, size_t count, cudaStream_t st, cudaGraph_t *capture = nullptr) {
+    arena_reset();
+    std::vector<uint64_t> ba(count), bb(count);
+    std::vector<int> sq(count), meth(count);
+    for (size_t i = 0; i < count; i++) {
+        ba[i] = jobs[i].bits_a;
+        sq[i] = jobs[i].square != 0;
+        bb[i] = sq[i] ? jobs[i].bits_a : jobs[i].bits_b;
+        meth[i] = jobs[i].method;
+    }
+    int rc = learned_resolve(ba.data(), bb.data(), sq.data(), meth.data(), count, st);
+    if (rc) return rc;
+    std::vector<BJob> bj;
+    bj.reserve(count);
+    for (size_t i = 0; i < count; i++) {
+        ffg_job &u = jobs[i];
+        const uint64_t nb = u.square ? u.na : u.nb;
+        if (ba[i] == 0 || bb[i] == 0) {
+            CK(cudaMemsetAsync(u.out, 0, (u.na + nb + 1) * 8, st));
+            continue;
+        }
+        BJob J{u.a, u.square ? u.a : u.b, u.na, nb, ba[i], bb[i], u.out, sq[i], 0, {}};
+        rc = method_plan(meth[i], ba[i], bb[i], sq[i], &J);
+        if (rc) return rc;
+        bj.push_back(J);
+    }
+    return run_batch(bj, st, capture);
 }
 
 extern "C" int ffg_mul_batch_device(ffg_job *jobs, size_t count, void *stream) {
@@ -1409,22 +1628,35 @@ extern "C" int ffg_mul_batch_device(ffg_job *jobs, size_t count, void *stream) {
     if (!jobs && count) return fail(FFG_E_ARG, "jobs is NULL");
     cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
     CK(cudaStreamSynchronize(st));
-    arena_reset();
-    std::vector<BJob> bj;
-    bj.reserve(count);
-    for (size_t i = 0; i < count; i++) {
-        ffg_job &u = jobs[i];
-        const uint64_t nb = u.square ? u.na : u.nb, bb = u.square ? u.bits_a : u.bits_b;
-        if (u.bits_a == 0 || bb == 0) {
-            CK(cudaMemsetAsync(u.out, 0, (u.na + nb + 1) * 8, st));
-            continue;
-        }
-        BJob J{u.a, u.square ? u.a : u.b, u.na, nb, u.bits_a, bb, u.out, u.square != 0, 0, {}};
-        rc = method_plan(u.method, u.bits_a, bb, u.square != 0, &J);
-        if (rc) return rc;
-        bj.push_back(J);
-    }
-    return run_batch(bj, st);
+    return batch_device_core(jobs, count, st);
+}
+
+extern "C" int ffg_time_batch(ffg_job *jobs, size_t count, int reps, double *ms) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if ((!jobs && count) || reps < 1 || !ms) return fail(FFG_E_ARG, "ffg_time_batch arguments");
+    cudaStream_t st = g.stream;
+    CK(cudaStreamSynchronize(st));
+    // the batch's launches captured once and replayed: device time only
+    // (plans and job uploads stay outside the clock)
+    cudaGraph_t gr = nullptr;
+    if ((rc = batch_device_core(jobs, count, st, &gr))) return rc;
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e) return fail(FFG_E_CUDA, "batch graph: %s", cudaGetErrorString(e));
+    e = cudaGraphLaunch(ex, st); // warm-up
+    if (!e) e = cudaEventRecord(g.ev0, st);
+    for (int r = 0; r < reps && !e; r++) e = cudaGraphLaunch(ex, st);
+    if (!e) e = cudaEventRecord(g.ev1, st);
+    if (!e) e = cudaEventSynchronize(g.ev1);
+    float t = 0;
+    if (!e) e = cudaEventElapsedTime(&t, g.ev0, g.ev1);
+    cudaGraphExecDestroy(ex);
+    if (e) return fail(FFG_E_CUDA, "batch timing: %s", cudaGetErrorString(e));
+    *ms = t / reps;
+    return FFG_OK;
 }
 
 extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
@@ -1465,6 +1697,13 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
         }
     }
     CK(cudaMemcpyAsync(din, hin, in_limbs * 8, cudaMemcpyHostToDevice, st));
+    std::vector<int> sqv(count), meth(count);
+    for (size_t i = 0; i < count; i++) sqv[i] = jobs[i].square != 0, meth[i] = jobs[i].method;
+    rc = learned_resolve(ba.data(), bb.data(), sqv.data(), meth.data(), count, st);
+    if (rc) {
+        pinned_release(hin);
+        return rc;
+    }
     std::vector<BJob> bj;
     for (size_t i = 0; i < count; i++) {
         if (ba[i] == 0 || bb[i] == 0) {
@@ -1472,7 +1711,7 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
             continue;
         }
         BJob J{din + aoff[i], din + boff[i], na[i], nb[i], ba[i], bb[i], dout + roff[i], jobs[i].square != 0, 0, {}};
-        rc = method_plan(jobs[i].method, ba[i], bb[i], jobs[i].square != 0, &J);
+        rc = method_plan(meth[i], ba[i], bb[i], jobs[i].square != 0, &J);
         if (rc) {
             pinned_release(hin);
             return rc;
@@ -1504,4 +1743,172 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
     pinned_release(hout);
     if (e) return fail(FFG_E_CUDA, "batch: %s", cudaGetErrorString(e));
     return FFG_OK;
+}
+
+// ------------------------------------------------------------ cost model ABI
+
+extern "C" int ffg_mlp_features(uint64_t bits_a, uint64_t bits_b, int square, float *f) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (!f) return fail(FFG_E_ARG, "f is NULL");
+    mlp_features(bits_a, bits_b, square, f);
+    return FFG_OK;
+}
+
+// Device copies of rows (X, method, y) in the arena.
+static int mlp_upload(const float *X, const int32_t *M, const float *Y, size_t n, float **dX, int32_t **dM, float **dY,
+                      cudaStream_t st) {
+    *dX = (float *)arena_alloc(std::max<size_t>(1, n) * FFG_MLP_D * sizeof(float));
+    *dM = (int32_t *)arena_alloc(std::max<size_t>(1, n) * sizeof(int32_t));
+    *dY = (float *)arena_alloc(std::max<size_t>(1, n) * sizeof(float));
+    if (!*dX || !*dM || !*dY) return fail(FFG_E_NOMEM, "device arena: training rows");
+    for (size_t i = 0; i < n; i++)
+        if (M[i] < 0 || M[i] >= FFG_MLP_K) return fail(FFG_E_ARG, "row %zu: method %d", i, (int)M[i]);
+    if (n) {
+        CK(cudaMemcpyAsync(*dX, X, n * FFG_MLP_D * sizeof(float), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(*dM, M, n * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(*dY, Y, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    }
+    return FFG_OK;
+}
+
+extern "C" int ffg_mlp_train(float *params, const float *X, const int32_t *method, const float *y, size_t n, int epochs,
+                             float lr, float *loss_hist) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!params || (!n && epochs > 0) || epochs < 0 || (n && (!X || !method || !y)))
+        return fail(FFG_E_ARG, "ffg_mlp_train arguments");
+    cudaStream_t st = g.stream;
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    float *dX, *dY;
+    int32_t *dM;
+    if ((rc = mlp_upload(X, method, y, n, &dX, &dM, &dY, st))) return rc;
+    float *dP = (float *)arena_alloc(FFG_MLP_NPARAM * sizeof(float));
+    float *dL = (float *)arena_alloc(std::max(1, epochs) * sizeof(float));
+    if (!dP || !dL) return fail(FFG_E_NOMEM, "device arena: parameters");
+    CK(cudaMemcpyAsync(dP, params, FFG_MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, st));
+    cudaError_t e = launch_mlp_train(dP, dX, dM, dY, (uint32_t)n, (uint32_t)epochs, lr, dL, st);
+    if (e) return fail(FFG_E_CUDA, "cost model training: %s", cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(params, dP, FFG_MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (loss_hist && epochs > 0) CK(cudaMemcpyAsync(loss_hist, dL, epochs * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return FFG_OK;
+}
+
+extern "C" int ffg_mlp_grad(const float *params, const float *X, const int32_t *method, const float *y, size_t n,
+                            float *grad, float *loss) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!params || !grad || !loss || !n || !X || !method || !y) return fail(FFG_E_ARG, "ffg_mlp_grad arguments");
+    cudaStream_t st = g.stream;
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    float *dX, *dY;
+    int32_t *dM;
+    if ((rc = mlp_upload(X, method, y, n, &dX, &dM, &dY, st))) return rc;
+    float *dP = (float *)arena_alloc(2 * FFG_MLP_NPARAM * sizeof(float) + 256), *dG = dP + FFG_MLP_NPARAM;
+    float *dL = (float *)arena_alloc(sizeof(float));
+    if (!dP || !dL) return fail(FFG_E_NOMEM, "device arena: parameters");
+    CK(cudaMemcpyAsync(dP, params, FFG_MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, st));
+    cudaError_t e = launch_mlp_grad(dP, dX, dM, dY, (uint32_t)n, dG, dL, st);
+    if (e) return fail(FFG_E_CUDA, "cost model gradient: %s", cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(grad, dG, FFG_MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(loss, dL, sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return FFG_OK;
+}
+
+extern "C" int ffg_mlp_predict(const float *params, const float *X, size_t n, float *out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if ((!params && g_mlp_host.empty()) || (n && (!X || !out))) return fail(FFG_E_ARG, "ffg_mlp_predict arguments");
+    cudaStream_t st = g.stream;
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    float *dX = (float *)arena_alloc(std::max<size_t>(1, n) * FFG_MLP_D * sizeof(float));
+    float *dO = (float *)arena_alloc(std::max<size_t>(1, n) * FFG_MLP_K * sizeof(float));
+    float *dP = params ? (float *)arena_alloc(FFG_MLP_NPARAM * sizeof(float)) : mlp_device();
+    if (!dX || !dO || !dP) return fail(FFG_E_NOMEM, "device arena: cost model rows");
+    if (params) CK(cudaMemcpyAsync(dP, params, FFG_MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, st));
+    if (n) CK(cudaMemcpyAsync(dX, X, n * FFG_MLP_D * sizeof(float), cudaMemcpyHostToDevice, st));
+    cudaError_t e = launch_mlp_infer(dP, dX, (uint32_t)n, dO, st);
+    if (e) return fail(FFG_E_CUDA, "cost model inference: %s", cudaGetErrorString(e));
+    if (n) CK(cudaMemcpyAsync(out, dO, n * FFG_MLP_K * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return FFG_OK;
+}
+
+extern "C" int ffg_mlp_set(const float *params) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (!params) {
+        g_mlp_host.clear();
+        return FFG_OK;
+    }
+    g_mlp_host.assign(params, params + FFG_MLP_NPARAM);
+    g_mlp_dirty = true;
+    return FFG_OK;
+}
+
+// ------------------------------------------------------------ tuning
+
+extern "C" int ffg_set_geometry(uint32_t lg, uint32_t r3, uint32_t row_lg, uint32_t wc) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (lg >= 32 || r3 > 1) return fail(FFG_E_ARG, "geometry: lg %u r3 %u", lg, r3);
+    if (row_lg == 0 && wc == 0) {
+        g_geo[lg][r3] = Geo{0, 0, 0};
+    } else {
+        if (!geo_valid(lg, r3, row_lg, wc)) return fail(FFG_E_ARG, "geometry lg %u r3 %u: c %u wc %u", lg, r3, row_lg, wc);
+        g_geo[lg][r3] = Geo{1, (uint8_t)row_lg, (uint8_t)wc};
+    }
+    chain_cache_clear(); // captured chains hold launches of the old geometry
+    return FFG_OK;
+}
+
+extern "C" int ffg_get_geometry(uint32_t lg, uint32_t r3, uint32_t *row_lg, uint32_t *wc) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (lg >= 32 || r3 > 1 || !row_lg || !wc) return fail(FFG_E_ARG, "geometry query");
+    ffg_plan pl{};
+    pl.lg = lg, pl.r3 = r3, pl.L = (uint64_t)(r3 ? 3 : 1) << lg, pl.split = 1; // split: always the four-step
+    gpu_geometry(&pl);
+    FourStep G = four_step_geometry(pl, true);
+    *row_lg = pl.row_lg;
+    *wc = G.wc;
+    return FFG_OK;
+}
+
+extern "C" int ffg_load_tuning(const char *path) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    FILE *f = path ? fopen(path, "r") : nullptr;
+    if (!f) return fail(FFG_E_ARG, "tuning file %s", path ? path : "(null)");
+    char word[32];
+    std::vector<float> params;
+    int rc = FFG_OK;
+    while (rc == FFG_OK && fscanf(f, "%31s", word) == 1) {
+        if (word[0] == '#') {
+            int ch;
+            while ((ch = fgetc(f)) != EOF && ch != '\n') {
+            }
+        } else if (!strcmp(word, "geometry")) {
+            unsigned lg, r3, c, wc;
+            if (fscanf(f, "%u %u %u %u", &lg, &r3, &c, &wc) != 4) rc = fail(FFG_E_ARG, "tuning: geometry line");
+            else rc = ffg_set_geometry(lg, r3, c, wc);
+        } else if (!strcmp(word, "mlp")) {
+            unsigned n;
+            if (fscanf(f, "%u", &n) != 1 || n != FFG_MLP_NPARAM) {
+                rc = fail(FFG_E_ARG, "tuning: mlp needs %d parameters", FFG_MLP_NPARAM);
+                break;
+            }
+            params.resize(n);
+            for (unsigned i = 0; i < n && rc == FFG_OK; i++)
+                if (fscanf(f, "%f", &params[i]) != 1) rc = fail(FFG_E_ARG, "tuning: mlp parameter %u", i);
+        } else {
+            rc = fail(FFG_E_ARG, "tuning: unknown entry %s", word);
+        }
+    }
+    fclose(f);
+    if (rc == FFG_OK && !params.empty()) rc = ffg_mlp_set(params.data());
+    return rc;
 }

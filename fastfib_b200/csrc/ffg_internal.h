@@ -81,6 +81,7 @@ struct CrtJob {
     uint32_t pad;
     int64_t add;
     uint32_t *maps;          // crt_ctas(nlimbs, width) words: each CTA's carry map
+    uint32_t *ticket;        // a zero word of the ticket pool (ticket_get)
 };
 
 // A linear combination out_k = alpha_k s1 + beta_k s2 + gamma_k over len limbs
@@ -94,6 +95,7 @@ struct LinJob {
     uint32_t nout;
     uint32_t pad;
     uint32_t *maps;          // 2 * lin_ctas(len) words: each CTA's carry map per output
+    uint32_t *ticket;        // a zero word of the ticket pool (ticket_get)
 };
 
 // Jobs travel to the kernels by value, as kernel parameters: nothing is
@@ -120,7 +122,16 @@ struct SchoolJob {
     uint64_t *out;
     uint64_t nlimbs;
     uint32_t *maps; // school_ctas(nlimbs) words
+    uint32_t *ticket; // a zero word of the ticket pool (ticket_get)
 };
+
+// Carries between the CTAs of one CRT, schoolbook product or linear pass are
+// settled inside the same launch: every CTA publishes its carry map, takes a
+// ticket (an atomic count on a word that is zero between launches), and the
+// CTA that draws the last ticket scans the maps, adds the carries and zeroes
+// the word again.  ticket_get hands out distinct words of a pool zeroed once;
+// launches captured into CUDA graphs draw from a region of their own.
+uint32_t *ticket_get();
 
 uint32_t crt_ctas(uint64_t nlimbs, uint32_t width); // CTAs (and carry maps) of one CRT
 __host__ __device__ uint32_t school_ctas(uint64_t nlimbs); // CTAs (and carry maps) of one schoolbook product
@@ -141,6 +152,13 @@ cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJobs &jo
 cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob &job, uint32_t pairs, cudaStream_t st);
 cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st);
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st);
+
+// The cost model's kernels (ffg_mlp.cu); parameters, rows and outputs on the device.
+cudaError_t launch_mlp_train(float *d_params, const float *d_X, const int32_t *d_M, const float *d_Y, uint32_t n,
+                             uint32_t epochs, float lr, float *d_loss_hist, cudaStream_t st);
+cudaError_t launch_mlp_grad(const float *d_params, const float *d_X, const int32_t *d_M, const float *d_Y, uint32_t n,
+                            float *d_grad, float *d_loss, cudaStream_t st);
+cudaError_t launch_mlp_infer(const float *d_params, const float *d_X, uint32_t n, float *d_out, cudaStream_t st);
 
 // Kernel families the profiler tracks (ffg_profile_read in include/ffg.h).
 enum ProfKind { PK_CONV_SMALL = 0, PK_COL_FWD, PK_ROW_CONV, PK_COL_INV, PK_CRT, PK_CARRY, PK_LIN, PK_SCHOOL, PK_COUNT };

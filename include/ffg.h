@@ -80,7 +80,11 @@ enum {
     FFG_M_SCHOOL = 0,   /* schoolbook (big_mul_schoolbook, src/bigint.c:257-276) */
     FFG_M_NTT = 1,      /* big_mul_ntt's plan (src/mul_ntt.c:97-118), the split past the cap */
     FFG_M_NTT_POW2 = 2, /* the same width, the transform length forced to 2^k */
-    FFG_M_NTT_R3 = 3    /* the same width, the transform length forced to 3 * 2^k */
+    FFG_M_NTT_R3 = 3,   /* the same width, the transform length forced to 3 * 2^k */
+    FFG_M_LEARNED = 4   /* the method of least predicted cost under the installed cost model
+                           (ffg_mlp_set) among FFG_M_SCHOOL..FFG_M_NTT_R3, taken only when
+                           predicted at least 10% cheaper than FFG_M_PLAIN's method; FFG_M_PLAIN
+                           without a model, and for products past the transform cap (the split) */
 };
 
 /* One product of a batch.  Device variant: a, b, out device pointers, out
@@ -104,6 +108,56 @@ typedef struct {
    src/decimal.c:177-203). */
 int ffg_mul_batch_device(ffg_job *jobs, size_t count, void *stream);
 int ffg_mul_batch_host(ffg_job *jobs, size_t count);
+
+/* The learned cost model (no counterpart in the reference, which dispatches
+   by fixed thresholds, src/mul_basic.c:30-38): an FP32 MLP
+     FFG_MLP_D features -> FFG_MLP_H (tanh) -> FFG_MLP_H (tanh) -> FFG_MLP_K
+   whose output m is the predicted log2 microseconds per product of method m
+   (FFG_M_SCHOOL .. FFG_M_NTT_R3) inside a batch.  Parameters, in order:
+   W1[H][D] b1[H] W2[H][H] b2[H] W3[K][H] b3[K].  Training, gradient and
+   inference run in CUDA kernels; a training row is (features, method,
+   measured log2 us), the loss half the mean squared error of the row's
+   method output. */
+#define FFG_MLP_D 8
+#define FFG_MLP_H 32
+#define FFG_MLP_K 4
+#define FFG_MLP_NPARAM                                                                                 \
+    (FFG_MLP_H * FFG_MLP_D + FFG_MLP_H + FFG_MLP_H * FFG_MLP_H + FFG_MLP_H + FFG_MLP_K * FFG_MLP_H + FFG_MLP_K)
+/* The features of a product of bit lengths bits_a, bits_b (host only). */
+int ffg_mlp_features(uint64_t bits_a, uint64_t bits_b, int square, float *f);
+/* Trains params (in: initial values, out: trained) on n rows for `epochs`
+   full-batch Adam steps of rate lr; loss_hist (NULL or epochs floats) gets the
+   loss before each step. */
+int ffg_mlp_train(float *params, const float *X, const int32_t *method, const float *y, size_t n, int epochs,
+                  float lr, float *loss_hist);
+/* One full-batch gradient (FFG_MLP_NPARAM floats) and the loss. */
+int ffg_mlp_grad(const float *params, const float *X, const int32_t *method, const float *y, size_t n, float *grad,
+                 float *loss);
+/* Every output for n feature rows (n * FFG_MLP_K floats); params NULL: the
+   installed model. */
+int ffg_mlp_predict(const float *params, const float *X, size_t n, float *out);
+/* Installs params for FFG_M_LEARNED (copied; sent to the GPU on first use,
+   so it works before any device exists); NULL removes the model. */
+int ffg_mlp_set(const float *params);
+/* Device milliseconds of the launches of one ffg_mul_batch_device call on
+   `jobs`: planned and uploaded once, its launches captured as a CUDA graph
+   and replayed reps times after one warm-up (the autotuner's clock; the
+   host's planning is not timed).  Products past the transform cap (the
+   split) are refused. */
+int ffg_time_batch(ffg_job *jobs, size_t count, int reps, double *ms);
+
+/* Tuned four-step geometry for transform length 2^lg (r3 0) or 3 * 2^lg
+   (r3 1): rows of 2^row_lg words and column tiles of wc columns (the
+   reference's fixed pass shapes, src/ntt_conv.c:158-226, have no tuned
+   counterpart).  row_lg = wc = 0 restores the default rule.  Captured
+   chains are dropped (they hold the old launches). */
+int ffg_set_geometry(uint32_t lg, uint32_t r3, uint32_t row_lg, uint32_t wc);
+/* The geometry in force for that length. */
+int ffg_get_geometry(uint32_t lg, uint32_t r3, uint32_t *row_lg, uint32_t *wc);
+/* Loads an autotuner file: lines "geometry lg r3 row_lg wc" and one line
+   "mlp N p0 .. p(N-1)" (the cost model, installed as by ffg_mlp_set);
+   "#" starts a comment. */
+int ffg_load_tuning(const char *path);
 
 /* No counterpart in the reference.  ffg_mul_device without any device
    allocation, for callers that cannot allocate once running: code issuing

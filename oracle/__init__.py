@@ -139,6 +139,37 @@ class Oracle(_Lib):
         self.lib.fo_mul_ntt_forced.argtypes = [_u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, ctypes.c_int,
                                                ctypes.c_uint32, ctypes.c_uint64, _szp]
 
+    def mlp_nparam(self) -> int:
+        self.lib.fo_mlp_nparam.restype = ctypes.c_size_t
+        return self.lib.fo_mlp_nparam()
+
+    def mlp_predict(self, params: np.ndarray, X: np.ndarray) -> np.ndarray:
+        """Every output of the cost model for the rows of X (float32, n x 8)."""
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.zeros((X.shape[0], 4), dtype=np.float64)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.lib.fo_mlp_predict.argtypes = [fp, fp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)]
+        self.lib.fo_mlp_predict(params.ctypes.data_as(fp), X.ctypes.data_as(fp), X.shape[0],
+                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
+
+    def mlp_grad(self, params: np.ndarray, X: np.ndarray, method: np.ndarray, y: np.ndarray):
+        """(loss, gradient) of the cost model in double precision."""
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        method = np.ascontiguousarray(method, dtype=np.int32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        grad = np.zeros(self.mlp_nparam(), dtype=np.float64)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.lib.fo_mlp_grad.argtypes = [fp, fp, ctypes.POINTER(ctypes.c_int32), fp, ctypes.c_size_t,
+                                         ctypes.POINTER(ctypes.c_double)]
+        self.lib.fo_mlp_grad.restype = ctypes.c_double
+        loss = self.lib.fo_mlp_grad(params.ctypes.data_as(fp), X.ctypes.data_as(fp),
+                                    method.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), y.ctypes.data_as(fp),
+                                    X.shape[0], grad.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return loss, grad
+
     def set_max_lg(self, lg: int) -> None:
         self.lib.fo_set_max_lg(lg)
 

@@ -50,6 +50,14 @@ char *fo_to_string(const uint64_t *a, size_t na);
 void fo_fingerprint(const uint64_t *a, size_t na, uint64_t out[6]);
 void fo_free(void *p);
 
+/* The learned dispatch's cost model (mlp_oracle.c): parameter count, every
+   output for n feature rows (n * 4 doubles), and the loss with its gradient
+   (fo_mlp_nparam() doubles). */
+size_t fo_mlp_nparam(void);
+void fo_mlp_predict(const float *params, const float *X, size_t n, double *out);
+double fo_mlp_grad(const float *params, const float *X, const int32_t *method, const float *y, size_t n,
+                   double *grad);
+
 #ifdef __cplusplus
 }
 #endif
