@@ -109,6 +109,10 @@ def lib() -> ctypes.CDLL:
     L.ffg_get_geometry.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
                                    ctypes.POINTER(ctypes.c_uint32)]
     L.ffg_load_tuning.argtypes = [ctypes.c_char_p]
+    L.ffg_to_decimal_host.argtypes = [_u64p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p), _szp,
+                                      ctypes.POINTER(ctypes.c_int)]
+    L.ffg_to_decimal_device.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p), _szp,
+                                        ctypes.POINTER(ctypes.c_int)]
     L.ffg_mul_batch_device.argtypes = [ctypes.POINTER(Job), ctypes.c_size_t, ctypes.c_void_p]
     L.ffg_release.argtypes = [ctypes.c_void_p]
     for name in ("big_mul", "big_mul_ntt", "big_mul_toom3"):
@@ -225,6 +229,23 @@ def big_to_string(a) -> str:
     s = ctypes.string_at(p).decode()
     ctypes.CDLL(None).free(ctypes.c_void_p(p))
     return s
+
+
+def to_decimal(a, device_ptr: int = 0, n: int = 0):
+    """ffg_to_decimal_host (or _device with device_ptr, n limbs): (digits,
+    True) from the device path, or (None, False) when it declined."""
+    out, nout, done = ctypes.c_void_p(), ctypes.c_size_t(), ctypes.c_int()
+    if device_ptr:
+        _check(lib().ffg_to_decimal_device(device_ptr, n, ctypes.byref(out), ctypes.byref(nout), ctypes.byref(done)))
+    else:
+        a = _arr(a)
+        _check(lib().ffg_to_decimal_host(a.ctypes.data_as(_u64p), a.size, ctypes.byref(out), ctypes.byref(nout),
+                                         ctypes.byref(done)))
+    if not done.value:
+        return None, False
+    s = ctypes.string_at(out.value, nout.value).decode()
+    ctypes.CDLL(None).free(out)
+    return s, True
 
 
 # ------------------------------------------------------------------ the GPU ABI

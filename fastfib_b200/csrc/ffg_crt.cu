@@ -40,9 +40,6 @@ FFG_DEV_INLINE uint32_t crt_ctas_dev(uint64_t nlimbs, uint32_t width) {
 }
 
 FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t cta);
-FFG_DEV_INLINE void settle_cta(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *maps,
-                               uint32_t ncta);
-FFG_DEV_INLINE bool last_cta(uint32_t *ticket, uint32_t ncta);
 
 __global__ void __launch_bounds__(CRT_THREADS) k_crt(GarnerConst K, CrtJob J) { crt_block(K, J, blockIdx.x); }
 
@@ -147,59 +144,6 @@ FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t ct
         settle_cta(J.out, J.nlimbs, NL, J.maps, ncta);
         if (threadIdx.x == 0) *J.ticket = 0;
     }
-}
-
-// Carries between CTAs, settled by the CTA that finishes last (all of its
-// threads): thread t composes the maps of its run of consecutive CTAs, a
-// block-wide scan of those composites gives the carry into every run (carry
-// 0 into the first CTA), and each thread walks its run again adding the
-// carry into the CTAs that receive one (a carry stops at the first limb that
-// does not wrap).  Maps and limbs written by other CTAs are read through L2.
-FFG_DEV_INLINE void settle_cta(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *maps,
-                               uint32_t ncta) {
-    __shared__ uint32_t wpre[32];
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const uint32_t per = (ncta + blockDim.x - 1) / blockDim.x;
-    const uint32_t q0 = min(ncta, threadIdx.x * per), q1 = min(ncta, q0 + per);
-    uint32_t run = 2u; // identity: c -> c
-    for (uint32_t q = q0; q < q1; q++) run = map_then(run, __ldcg(&maps[q]));
-    const uint32_t inc = warp_map_scan(run);
-    if (lane == 31) wpre[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t v = warp_map_scan(lane < nw ? wpre[lane] : 2u);
-        __syncwarp();
-        if (lane < nw) wpre[lane] = v;
-    }
-    __syncthreads();
-    uint32_t exc = __shfl_up_sync(0xffffffffu, inc, 1);
-    if (lane == 0) exc = 2u;
-    const uint32_t before = warp ? map_then(wpre[warp - 1], exc) : exc;
-    uint32_t carry = map_apply(before, 0);
-    for (uint32_t q = q0; q < q1; q++) {
-        if (carry) {
-            const uint64_t end = min(nlimbs, (uint64_t)(q + 1) * cta_limbs);
-            for (uint64_t j = (uint64_t)q * cta_limbs; j < end; j++) {
-                const uint64_t v = __ldcg(&out[j]) + 1;
-                out[j] = v;
-                if (v != 0) break;
-            }
-        }
-        carry = map_apply(__ldcg(&maps[q]), carry);
-    }
-    __syncthreads();
-}
-
-// Called by every CTA of a launch after its limbs and map are written:
-// true in the one CTA that takes the last of ncta tickets.
-FFG_DEV_INLINE bool last_cta(uint32_t *ticket, uint32_t ncta) {
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == ncta - 1;
-    __syncthreads();
-    if (last) __threadfence();
-    return last;
 }
 
 uint32_t crt_ctas(uint64_t nlimbs, uint32_t width) {

@@ -75,6 +75,7 @@ struct Ctx {
 
 static Ctx g;
 static std::recursive_mutex g_mu;
+static void dec_free();
 
 // ------------------------------------------------------------ ticket pool
 
@@ -1471,6 +1472,7 @@ extern "C" void ffg_shutdown(void) {
     g_mlp = nullptr;
     if (g_tickets) cudaFree(g_tickets);
     g_tickets = nullptr;
+    dec_free();
     for (auto &b : g_pinned_pool) cudaFreeHost(b.first);
     g_pinned_pool.clear();
     cudaEventDestroy(g.ev0);
@@ -1910,5 +1912,371 @@ extern "C" int ffg_load_tuning(const char *path) {
     }
     fclose(f);
     if (rc == FFG_OK && !params.empty()) rc = ffg_mlp_set(params.data());
+    return rc;
+}
+
+// =================================================== decimal conversion
+//
+// big_to_string (src/decimal.c:229-281) on the device, breadth first.  With
+// P_l = 10^(19 2^l) of exactly s_l bits and T the least level with
+// 2 (s_T - 1) >= bits(x), level l splits every piece x < 2^(2 s_l) into
+// q = floor(x / P_l) and r = x mod P_l by Barrett's method
+//     q1 = x >> (s - 1),  q = (q1 m) >> (s + 1),  m <= floor(2^(2s) / P)
+// (src/decimal.c:76-89), then one correction: k = floor((x - q P) / P) from
+// 64-bit windows (k_khat_batch, exact or one too large), r = x - q P - k P,
+// q += k (k_comb_batch).  All pieces of a level share each launch: two
+// shifts, two batched products (grouped by plan, src/decimal.c:177-203 does
+// them one at a time), the estimate and one combination.  Pieces below
+// 10^(19 2^(leaf + 1)) become 19 2^(leaf + 1) digits each (k_leaf_digits,
+// the reference's dec_leaf, src/decimal.c:139-150); leading zeros are
+// dropped on the host.  An estimate out of its range (which the bounds rule
+// out) raises a flag and the conversion is redone on the host path.
+//
+// The powers and their reciprocals depend only on the level; they stay on
+// the device between calls.  The reciprocals come from Newton's iteration
+// from below (src/decimal.c:39-71 restated so that every sign is known):
+//     y' = y + floor(y (2^(2s) - P y) / 2^(2s))  <=  floor(2^(2s) / P),
+// started at level l from (m_(l-1))^2 >> (4 s_(l-1) - 2 s_l), two steps a
+// level (the error of the start squares twice to a few units).
+
+namespace ffg {
+
+static const int kDecLeafLg = 4; // DEC_LEAF_LG (src/decimal.c): leaves below 10^(19 * 32)
+static const uint64_t kDec19 = 10000000000000000000ull;
+
+struct DecLevel {
+    uint64_t *P = nullptr, *m = nullptr; // dedicated allocations (kept between calls)
+    uint64_t nP = 0, nm = 0;
+    uint64_t s = 0;                      // bits of P
+};
+static std::vector<DecLevel> g_dec;
+
+static uint64_t limbs_of(uint64_t bits) { return std::max<uint64_t>(1, (bits + 63) / 64); }
+
+// Device helpers on stream st, temporaries from the arena.
+static int dev_upload_jobs(const void *h, size_t bytes, void **d, cudaStream_t st) {
+    *d = arena_alloc(std::max<size_t>(bytes, 16));
+    if (!*d) return fail(FFG_E_NOMEM, "device arena: job records");
+    if (bytes) CK(cudaMemcpyAsync(*d, h, bytes, cudaMemcpyHostToDevice, st));
+    return FFG_OK;
+}
+
+static int dev_shift(std::vector<ShiftJob> &jobs, cudaStream_t st) {
+    if (jobs.empty()) return FFG_OK;
+    uint64_t mx = 0;
+    for (auto &j : jobs) mx = std::max(mx, j.nout);
+    void *d;
+    int rc = dev_upload_jobs(jobs.data(), jobs.size() * sizeof(ShiftJob), &d, st);
+    if (rc) return rc;
+    cudaError_t e = launch_shift_batch((const ShiftJob *)d, (uint32_t)jobs.size(), mx, st);
+    return e ? fail(FFG_E_CUDA, "decimal shift: %s", cudaGetErrorString(e)) : FFG_OK;
+}
+
+static int dev_comb(std::vector<CombJob> &jobs, cudaStream_t st) {
+    if (jobs.empty()) return FFG_OK;
+    uint64_t mx = 0;
+    for (auto &j : jobs) {
+        mx = std::max(mx, j.len);
+        j.maps = (uint32_t *)arena_alloc((size_t)comb_ctas(j.len) * 4);
+        if (!j.maps) return fail(FFG_E_NOMEM, "device arena: combination maps");
+        j.ticket = ticket_get();
+    }
+    void *d;
+    int rc = dev_upload_jobs(jobs.data(), jobs.size() * sizeof(CombJob), &d, st);
+    if (rc) return rc;
+    cudaError_t e = launch_comb_batch((const CombJob *)d, (uint32_t)jobs.size(), mx, st);
+    return e ? fail(FFG_E_CUDA, "decimal combination: %s", cudaGetErrorString(e)) : FFG_OK;
+}
+
+// Products out_i = a_i b_i (out_i: na + nb + 1 limbs), the plain thresholds.
+static int dev_products(std::vector<BJob> &jobs, cudaStream_t st) {
+    std::vector<BJob> run;
+    for (BJob J : jobs) {
+        const int rc = method_plan(FFG_M_PLAIN, J.bits_a, J.bits_b, J.square, &J);
+        if (rc) return rc;
+        run.push_back(J);
+    }
+    return run_batch(run, st);
+}
+
+static BJob bjob(const uint64_t *a, uint64_t na, uint64_t ba, const uint64_t *b, uint64_t nb, uint64_t bb, uint64_t *out,
+                 bool square) {
+    BJob J{};
+    J.a = a, J.b = square ? a : b, J.na = na, J.nb = square ? na : nb;
+    J.bits_a = std::min(ba, 64 * na), J.bits_b = square ? J.bits_a : std::min(bb, 64 * nb);
+    J.out = out, J.square = square;
+    return J;
+}
+
+static uint32_t top_bits_of(uint64_t bits) { return (uint32_t)(bits & 63); }
+
+// One Newton step from below for m ~ 2^(2s) / P (y: ny limbs, at most s + 1 bits;
+// ynew: limbs_of(s + 1)).
+static int newton_step(const DecLevel &L, const uint64_t *y, uint64_t ny, uint64_t *ynew, cudaStream_t st) {
+    const uint64_t s = L.s, len2 = limbs_of(2 * s);
+    uint64_t *d = (uint64_t *)arena_alloc((L.nP + ny + 1) * 8);
+    uint64_t *e = (uint64_t *)arena_alloc(len2 * 8);
+    uint64_t *u = (uint64_t *)arena_alloc((ny + len2 + 1) * 8);
+    uint64_t *w = (uint64_t *)arena_alloc(limbs_of(s + 1) * 8);
+    if (!d || !e || !u || !w) return fail(FFG_E_NOMEM, "device arena: Newton step");
+    std::vector<BJob> p1{bjob(L.P, L.nP, s, y, ny, s + 1, d, false)};
+    int rc = dev_products(p1, st);
+    if (rc) return rc;
+    // e = 2^(2s) - P y: two's complement over 2s bits (0 < P y < 2^(2s))
+    CombJob c{};
+    c.src[0] = d, c.n[0] = std::min<uint64_t>(L.nP + ny + 1, len2), c.mul[0] = -1;
+    c.out = e, c.len = len2, c.top_bits = top_bits_of(2 * s);
+    std::vector<CombJob> cj{c};
+    if ((rc = dev_comb(cj, st))) return rc;
+    std::vector<BJob> p2{bjob(y, ny, s + 1, e, len2, 2 * s, u, false)};
+    if ((rc = dev_products(p2, st))) return rc;
+    std::vector<ShiftJob> sj{ShiftJob{u, ny + len2 + 1, w, limbs_of(s + 1), 2 * s}};
+    if ((rc = dev_shift(sj, st))) return rc;
+    CombJob c2{};
+    c2.src[0] = y, c2.n[0] = ny, c2.mul[0] = 1;
+    c2.src[1] = w, c2.n[1] = limbs_of(s + 1), c2.mul[1] = 1;
+    c2.out = ynew, c2.len = limbs_of(s + 1);
+    std::vector<CombJob> cj2{c2};
+    return dev_comb(cj2, st);
+}
+
+static void dec_free() {
+    for (auto &L : g_dec) {
+        if (L.P) cudaFree(L.P);
+        if (L.m) cudaFree(L.m);
+    }
+    g_dec.clear();
+}
+
+// Levels 0..T of powers and reciprocals (kept between calls).
+static int dec_prepare(int T, cudaStream_t st) {
+    while ((int)g_dec.size() <= T) {
+        const int l = (int)g_dec.size();
+        DecLevel L;
+        if (l == 0) {
+            L.s = 64, L.nP = 1, L.nm = 2;
+            CK(cudaMalloc(&L.P, 8));
+            CK(cudaMalloc(&L.m, 16));
+            const uint64_t m0[2] = {(uint64_t)((~(u128h)0) / kDec19), (uint64_t)(((~(u128h)0) / kDec19) >> 64)};
+            CK(cudaMemcpy(L.P, &kDec19, 8, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(L.m, m0, 16, cudaMemcpyHostToDevice));
+            g_dec.push_back(L);
+            continue;
+        }
+        const DecLevel &B = g_dec[l - 1];
+        CK(cudaStreamSynchronize(st));
+        arena_reset();
+        const uint64_t nsq = 2 * B.nP + 1;
+        CK(cudaMalloc(&L.P, nsq * 8));
+        std::vector<BJob> sq{bjob(B.P, B.nP, B.s, nullptr, 0, 0, L.P, true)};
+        int rc = dev_products(sq, st);
+        if (rc) return rc;
+        uint64_t *dbits = (uint64_t *)arena_alloc(8);
+        if (!dbits) return fail(FFG_E_NOMEM, "device arena: bit length");
+        cudaError_t e = launch_bit_length(L.P, nsq, dbits, st);
+        if (e) return fail(FFG_E_CUDA, "decimal powers: %s", cudaGetErrorString(e));
+        CK(cudaMemcpyAsync(&L.s, dbits, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        L.nP = limbs_of(L.s);
+        // m: start from the previous level's reciprocal squared, two Newton steps
+        L.nm = limbs_of(L.s + 1);
+        CK(cudaMalloc(&L.m, L.nm * 8));
+        uint64_t *sqm = (uint64_t *)arena_alloc((2 * B.nm + 1) * 8);
+        uint64_t *y0 = (uint64_t *)arena_alloc(L.nm * 8), *y1 = (uint64_t *)arena_alloc(L.nm * 8);
+        if (!sqm || !y0 || !y1) return fail(FFG_E_NOMEM, "device arena: reciprocal");
+        std::vector<BJob> msq{bjob(B.m, B.nm, B.s + 1, nullptr, 0, 0, sqm, true)};
+        if ((rc = dev_products(msq, st))) return rc;
+        std::vector<ShiftJob> sh{ShiftJob{sqm, 2 * B.nm + 1, y0, L.nm, 4 * B.s - 2 * L.s}};
+        if ((rc = dev_shift(sh, st))) return rc;
+        g_dec.push_back(L); // newton_step reads P and s through it
+        DecLevel &N = g_dec.back();
+        if ((rc = newton_step(N, y0, N.nm, y1, st))) return rc;
+        if ((rc = newton_step(N, y1, N.nm, N.m, st))) return rc;
+        CK(cudaStreamSynchronize(st));
+    }
+    return FFG_OK;
+}
+
+// The conversion proper; *err_flag set on the device when a correction fell
+// outside its range (the caller then converts on the host path).
+static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, size_t *nout, bool *fallback,
+                      cudaStream_t st) {
+    *fallback = false;
+    int T = 0;
+    // powers as needed for the choice of T
+    while (true) {
+        int rc = dec_prepare(T, st);
+        if (rc) return rc;
+        if (2 * (g_dec[T].s - 1) >= bx) break;
+        T++;
+    }
+    if (T <= kDecLeafLg + 1) {
+        *fallback = true; // small numbers: the host path
+        return FFG_OK;
+    }
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    uint32_t *flag = (uint32_t *)arena_alloc(4);
+    uint64_t *one = (uint64_t *)arena_alloc(8);
+    if (!flag || !one) return fail(FFG_E_NOMEM, "device arena: flag");
+    CK(cudaMemsetAsync(flag, 0, 4, st));
+    const uint64_t h_one = 1;
+    CK(cudaMemcpyAsync(one, &h_one, 8, cudaMemcpyHostToDevice, st));
+    // pieces of the current level: pointer, limbs, bit bound
+    struct Piece {
+        const uint64_t *d;
+        uint64_t n, bits;
+    };
+    std::vector<Piece> cur{Piece{x, nx, bx}};
+    for (int l = T; l > kDecLeafLg; l--) {
+        const DecLevel &L = g_dec[l];
+        const uint64_t s = L.s, cnt = cur.size();
+        const uint64_t nq1 = limbs_of(s + 1), nt = nq1 + L.nm + 1, nq = limbs_of(s + 1), nqp = nq + L.nP + 1;
+        const uint64_t nr = limbs_of(s + 1), nqo = limbs_of(s + 1);
+        uint64_t *q1 = (uint64_t *)arena_alloc(cnt * nq1 * 8), *t = (uint64_t *)arena_alloc(cnt * nt * 8);
+        uint64_t *q = (uint64_t *)arena_alloc(cnt * nq * 8), *qp = (uint64_t *)arena_alloc(cnt * nqp * 8);
+        uint32_t *kh = (uint32_t *)arena_alloc(cnt * 4), *sg = (uint32_t *)arena_alloc(cnt * 4);
+        uint64_t *r1 = (uint64_t *)arena_alloc(cnt * nr * 8);
+        uint64_t *r = (uint64_t *)arena_alloc(cnt * nr * 8), *qo = (uint64_t *)arena_alloc(cnt * nqo * 8);
+        if (!q1 || !t || !q || !qp || !kh || !sg || !r1 || !r || !qo)
+            return fail(FFG_E_NOMEM, "device arena: decimal level %d", l);
+        std::vector<ShiftJob> sh;
+        std::vector<BJob> pr;
+        for (uint64_t p = 0; p < cnt; p++) sh.push_back(ShiftJob{cur[p].d, cur[p].n, q1 + p * nq1, nq1, s - 1});
+        int rc = dev_shift(sh, st);
+        if (rc) return rc;
+        for (uint64_t p = 0; p < cnt; p++)
+            pr.push_back(bjob(q1 + p * nq1, nq1, s + 1, L.m, L.nm, s + 1, t + p * nt, false));
+        if ((rc = dev_products(pr, st))) return rc;
+        sh.clear();
+        for (uint64_t p = 0; p < cnt; p++) sh.push_back(ShiftJob{t + p * nt, nt, q + p * nq, nq, s + 1});
+        if ((rc = dev_shift(sh, st))) return rc;
+        pr.clear();
+        for (uint64_t p = 0; p < cnt; p++) pr.push_back(bjob(q + p * nq, nq, s + 1, L.P, L.nP, s, qp + p * nqp, false));
+        if ((rc = dev_products(pr, st))) return rc;
+        std::vector<KhatJob> kj;
+        for (uint64_t p = 0; p < cnt; p++)
+            kj.push_back(KhatJob{cur[p].d, qp + p * nqp, L.P, cur[p].n, nqp, L.nP, s, kh + p, flag});
+        void *dk;
+        if ((rc = dev_upload_jobs(kj.data(), kj.size() * sizeof(KhatJob), &dk, st))) return rc;
+        cudaError_t e = launch_khat_batch((const KhatJob *)dk, (uint32_t)cnt, st);
+        if (e) return fail(FFG_E_CUDA, "decimal estimate: %s", cudaGetErrorString(e));
+        // r1 = x - q P - k P over s + 1 bits (negative when k is one too
+        // large: then r1 + P and q + k - 1), its sign per piece
+        std::vector<CombJob> cj;
+        for (uint64_t p = 0; p < cnt; p++) {
+            CombJob c{};
+            c.src[0] = cur[p].d, c.n[0] = std::min(cur[p].n, nr), c.mul[0] = 1;
+            c.src[1] = qp + p * nqp, c.n[1] = std::min(nqp, nr), c.mul[1] = -1;
+            c.src[2] = L.P, c.n[2] = std::min(L.nP, nr), c.mul[2] = -1, c.scale[2] = kh + p;
+            c.out = r1 + p * nr, c.len = nr, c.sign_out = sg + p;
+            cj.push_back(c);
+        }
+        if ((rc = dev_comb(cj, st))) return rc;
+        cj.clear();
+        for (uint64_t p = 0; p < cnt; p++) {
+            CombJob c{}; // r = r1 + sign P
+            c.src[0] = r1 + p * nr, c.n[0] = nr, c.mul[0] = 1;
+            c.src[1] = L.P, c.n[1] = std::min(L.nP, nr), c.mul[1] = 1, c.scale[1] = sg + p;
+            c.out = r + p * nr, c.len = nr, c.neg_flag = flag;
+            cj.push_back(c);
+            CombJob d{}; // q + k - sign
+            d.src[0] = q + p * nq, d.n[0] = nq, d.mul[0] = 1, d.add_dev = kh + p;
+            d.src[1] = one, d.n[1] = 1, d.mul[1] = -1, d.scale[1] = sg + p;
+            d.out = qo + p * nqo, d.len = nqo;
+            cj.push_back(d);
+        }
+        if ((rc = dev_comb(cj, st))) return rc;
+        std::vector<Piece> nxt;
+        for (uint64_t p = 0; p < cnt; p++) {
+            nxt.push_back(Piece{qo + p * nqo, nqo, s});
+            nxt.push_back(Piece{r + p * nr, nr, s});
+        }
+        cur.swap(nxt);
+    }
+    // leaves: below P_(leaf + 1), 2 << leaf chunks of 19 digits each
+    const uint32_t chunks = 2u << kDecLeafLg;
+    std::vector<LeafJob> lj;
+    for (auto &p : cur) {
+        if (p.n > (uint64_t)FFG_LEAF_MAX_LIMBS) return fail(FFG_E_ARG, "decimal leaf of %llu limbs", (unsigned long long)p.n);
+        lj.push_back(LeafJob{p.d, p.n});
+    }
+    const uint64_t total = (uint64_t)lj.size() * chunks * 19;
+    char *dd = (char *)arena_alloc(total);
+    void *dl;
+    int rc = dd ? dev_upload_jobs(lj.data(), lj.size() * sizeof(LeafJob), &dl, st) : fail(FFG_E_NOMEM, "digits");
+    if (rc) return rc;
+    const uint64_t v = (uint64_t)((~(u128h)0) / kDec19 - ((u128h)1 << 64));
+    cudaError_t e = launch_leaf_digits((const LeafJob *)dl, (uint32_t)lj.size(), chunks, v, dd, st);
+    if (e) return fail(FFG_E_CUDA, "decimal leaves: %s", cudaGetErrorString(e));
+    char *h = (char *)malloc(total + 1);
+    if (!h) return fail(FFG_E_NOMEM, "host digits");
+    uint32_t hflag = 0;
+    CK(cudaMemcpyAsync(h, dd, total, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hflag) {
+        free(h);
+        *fallback = true;
+        return FFG_OK;
+    }
+    uint64_t z = 0;
+    while (z + 1 < total && h[z] == '0') z++;
+    memmove(h, h + z, total - z);
+    h[total - z] = 0;
+    *out = h;
+    *nout = total - z;
+    return FFG_OK;
+}
+
+} // namespace ffg
+
+// Decimal digits of the device number x (nx limbs) into a malloc'd string
+// (*out, *nout digits, NUL-terminated); *done 0 when the device path declined
+// (small numbers, or a correction out of range) and the caller must convert
+// on the host.
+extern "C" int ffg_to_decimal_device(const uint64_t *x, size_t nx, char **out, size_t *nout, int *done) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!x || !out || !nout || !done) return fail(FFG_E_ARG, "ffg_to_decimal_device arguments");
+    cudaStream_t st = g.stream;
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    uint64_t *dbits = (uint64_t *)arena_alloc(8), bx = 0;
+    if (!dbits) return fail(FFG_E_NOMEM, "device arena: bit length");
+    cudaError_t e = launch_bit_length(x, nx, dbits, st);
+    if (e) return fail(FFG_E_CUDA, "bit length: %s", cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(&bx, dbits, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    bool fallback = false;
+    *done = 0;
+    if (bx == 0) return FFG_OK;
+    rc = dec_device(x, limbs_of(bx), bx, out, nout, &fallback, st);
+    if (rc) return rc;
+    *done = fallback ? 0 : 1;
+    return FFG_OK;
+}
+
+extern "C" int ffg_to_decimal_host(const uint64_t *x, size_t nx, char **out, size_t *nout, int *done) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!x || !out || !nout || !done) return fail(FFG_E_ARG, "ffg_to_decimal_host arguments");
+    while (nx > 1 && x[nx - 1] == 0) nx--;
+    *done = 0;
+    if (nx == 1 && x[0] == 0) return FFG_OK;
+    CK(cudaStreamSynchronize(g.stream));
+    arena_reset();
+    // the number gets its own allocation: dec_device resets the arena
+    uint64_t *dx = nullptr;
+    CK(cudaMalloc(&dx, nx * 8));
+    cudaError_t e = cudaMemcpy(dx, x, nx * 8, cudaMemcpyHostToDevice);
+    if (e) {
+        cudaFree(dx);
+        return fail(FFG_E_CUDA, "decimal upload: %s", cudaGetErrorString(e));
+    }
+    rc = ffg_to_decimal_device(dx, nx, out, nout, done);
+    cudaFree(dx);
     return rc;
 }

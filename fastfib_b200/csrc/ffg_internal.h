@@ -133,6 +133,61 @@ struct SchoolJob {
 // launches captured into CUDA graphs draw from a region of their own.
 uint32_t *ticket_get();
 
+// ---------------------------------------------------- decimal conversion jobs
+
+// out = bits [shift, shift + 64 nout) of src (nsrc limbs, zero beyond).
+struct ShiftJob {
+    const uint64_t *src;
+    uint64_t nsrc;
+    uint64_t *out;
+    uint64_t nout;
+    uint64_t shift;
+};
+
+// out = sum over t of mul[t] (* *scale[t]) src[t] + add (+ *add_dev), mod
+// 2^(64 len); top_bits nonzero: the top limb keeps its low top_bits bits;
+// a negative result is one whose top limb ends with bit 63 set.
+struct CombJob {
+    const uint64_t *src[3];
+    uint64_t n[3];              // limbs of each source; 0: term unused
+    int32_t mul[3];
+    const uint32_t *scale[3];   // nullable
+    uint64_t *out;
+    uint64_t len;
+    int64_t add;
+    const uint32_t *add_dev;    // nullable
+    uint32_t top_bits;
+    uint32_t *neg_flag;         // nullable: raised (atomic or) on a negative result
+    uint32_t *sign_out;         // nullable: written 1 / 0 for a negative / non-negative result
+    uint32_t *maps;             // comb_ctas(len) words
+    uint32_t *ticket;
+};
+
+// khat = an estimate of floor((x - qp) / P) for P of s bits, exact or one
+// too large; flag raised if the estimate is out of range.
+struct KhatJob {
+    const uint64_t *x, *qp, *P;
+    uint64_t nx, nqp, nP;
+    uint64_t s;
+    uint32_t *khat;
+    uint32_t *flag;
+};
+
+// One leaf piece (below 10^(19 chunks)).
+constexpr int FFG_LEAF_MAX_LIMBS = 34;
+struct LeafJob {
+    const uint64_t *x;
+    uint64_t n;
+};
+
+__host__ __device__ uint32_t comb_ctas(uint64_t len);
+cudaError_t launch_shift_batch(const ShiftJob *d_jobs, uint32_t count, uint64_t max_out, cudaStream_t st);
+cudaError_t launch_comb_batch(const CombJob *d_jobs, uint32_t count, uint64_t max_len, cudaStream_t st);
+cudaError_t launch_khat_batch(const KhatJob *d_jobs, uint32_t count, cudaStream_t st);
+cudaError_t launch_leaf_digits(const LeafJob *d_jobs, uint32_t count, uint32_t chunks, uint64_t v, char *d_out,
+                               cudaStream_t st);
+cudaError_t launch_bit_length(const uint64_t *x, uint64_t n, uint64_t *d_out, cudaStream_t st);
+
 uint32_t crt_ctas(uint64_t nlimbs, uint32_t width); // CTAs (and carry maps) of one CRT
 __host__ __device__ uint32_t school_ctas(uint64_t nlimbs); // CTAs (and carry maps) of one schoolbook product
 // Batches in device arrays: one launch (plus one settle) for all products.

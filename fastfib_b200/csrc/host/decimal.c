@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include "fastfib.h"
+#include "ffg.h"
 #include "host_internal.h"
 
 #ifndef DEC_LEAF_LG
@@ -125,6 +126,10 @@ static void dec_emit(const DecCtx *c, Big x, int lvl, char *out) {
     dec_emit(c, r, lvl - 1, out + ((size_t)19 << lvl));
 }
 
+/* Numbers of at least this many bits convert on the device (ffg_to_decimal_host:
+   every level's Barrett products batched); smaller ones here. */
+#define DEC_DEVICE_BITS 16384
+
 char *big_to_string(const Big *a) {
     if (big_is_zero(a)) {
         char *s = malloc(2);
@@ -132,6 +137,14 @@ char *big_to_string(const Big *a) {
         s[0] = '0';
         s[1] = 0;
         return s;
+    }
+    if (big_bits(a) >= DEC_DEVICE_BITS) {
+        char *s = NULL;
+        size_t n = 0;
+        int done = 0;
+        if (ffg_to_decimal_host(a->d, a->n, &s, &n, &done)) ff_gpu_failed("decimal conversion", ffg_last_error());
+        if (done) return s;
+        /* declined (a correction out of range): the level-by-level path below */
     }
     DecCtx *c = xmalloc(sizeof(DecCtx));
     size_t ba = big_bits(a);

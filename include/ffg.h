@@ -146,6 +146,17 @@ int ffg_mlp_set(const float *params);
    split) are refused. */
 int ffg_time_batch(ffg_job *jobs, size_t count, int reps, double *ms);
 
+/* Decimal digits (big_to_string, src/decimal.c:229-281) of a number on the
+   device (x: device pointer) or on the host (x: host pointer), converted on
+   the device level by level: every level's Barrett products in shared
+   launches.  *out is a malloc'd NUL-terminated string of *nout digits (free
+   with free()).  *done = 0 when the device path declines -- numbers below
+   about 10^1200 and the rare case of a quotient correction out of range --
+   and the caller converts another way (big_to_string then uses its host
+   path). */
+int ffg_to_decimal_device(const uint64_t *x, size_t nx, char **out, size_t *nout, int *done);
+int ffg_to_decimal_host(const uint64_t *x, size_t nx, char **out, size_t *nout, int *done);
+
 /* Tuned four-step geometry for transform length 2^lg (r3 0) or 3 * 2^lg
    (r3 1): rows of 2^row_lg words and column tiles of wc columns (the
    reference's fixed pass shapes, src/ntt_conv.c:158-226, have no tuned

@@ -12,8 +12,9 @@ Sources (all produced here, none written by hand):
   reference built from its sources (oracle/_ref) AND, independently, the
   method of tests/fingerprint.py (fast doubling mod p, Binet with mpmath);
   the script refuses to write unless both agree.
-* Decimal digits of F(10^6) (sha256) from the reference's big_to_string,
-  checked against Python's str().
+* Decimal digits of F(10^6), F(10^7) and F(10^8) (sha256 and digit count)
+  from the reference's big_to_string, each checked against Python's str().
+  `--decimal-only` rewrites just that file.
 """
 import hashlib
 import json
@@ -77,8 +78,24 @@ def fingerprint_limbs(d):
     return out
 
 
+def decimal_golden(ref):
+    dec = {}
+    for n in (10**6, 10**7, 10**8):
+        f = ref.fibonacci(n)
+        s = ref.to_string(f)
+        assert s == str(limbs_to_int(f)), n
+        dec[str(n)] = hashlib.sha256(s.encode()).hexdigest()
+        dec[f"digits_{n}"] = len(s)
+        print("decimal", n, len(s), flush=True)
+    with open(os.path.join(HERE, "decimal_sha256.json"), "w") as f:
+        json.dump(dec, f, indent=1)
+
+
 def main():
     build(with_reference=True)
+    if "--decimal-only" in sys.argv:
+        decimal_golden(Reference())
+        return
     from fibonacci import fibonacci  # the reference's Python oracle (fibonacci.py)
     ref = Reference()
 
@@ -99,10 +116,6 @@ def main():
         fps[str(n)] = mine
         print("fingerprint", n, "ok", flush=True)
 
-    f6 = ref.fibonacci(10**6)
-    s = ref.to_string(f6)
-    assert s == str(limbs_to_int(f6))
-    dec = {"1000000": hashlib.sha256(s.encode()).hexdigest(), "digits_1000000": len(s)}
 
     with open(os.path.join(HERE, "fib_hex_sha256.json"), "w") as f:
         json.dump({"source": "fibonacci.py (reference) for tests/check.py's n list, seed 1", "sha256": hexes}, f,
@@ -110,8 +123,7 @@ def main():
     with open(os.path.join(HERE, "fingerprints.json"), "w") as f:
         json.dump({"primes": [str(p) for p in P4], "fields": ["bits", "low64", "mod_a", "mod_b", "mod_c", "mod_d"],
                    "fingerprints": {k: [str(v) for v in vals] for k, vals in fps.items()}}, f, indent=1)
-    with open(os.path.join(HERE, "decimal_sha256.json"), "w") as f:
-        json.dump(dec, f, indent=1)
+    decimal_golden(ref)
     print("written")
 
 
