@@ -119,8 +119,18 @@ def cpu_baseline(n, steps=7):
         t = time.perf_counter()
         run(n)
         best = min(best, time.perf_counter() - t)
-    return {"value": best * 1e3, "unit": "ms", "cores": cores, "kind": kind,
-            "sample": f"F({n}) best of {steps} runs after one warm-up, all pool threads"}
+    out = {"value": best * 1e3, "unit": "ms", "cores": cores, "kind": kind,
+           "sample": f"F({n}) best of {steps} runs after one warm-up, all pool threads"}
+    if kind == "reference":
+        f = run(n)
+        dec = float("inf")
+        for _ in range(3):
+            t = time.perf_counter()
+            ref.to_string(f)
+            dec = min(dec, time.perf_counter() - t)
+        out["decimal_ms"] = dec * 1e3
+        out["decimal_sample"] = f"big_to_string(F({n})) best of 3, all pool threads"
+    return out
 
 
 def run_reference(args, rank, world):
@@ -220,6 +230,32 @@ def run_ntt_microbench(args):
     return 0 if ok else 1
 
 
+def run_decimal(n=10**8, reps=3):
+    """Decimal digits of F(n) through the device conversion (the reference's
+    big_to_string, level by level with batched Barrett products): device ms
+    of the levels and leaves (powers and reciprocals cached after the first
+    call), wall ms of the host API call (number copied in, digits copied
+    out), the first call with the powers, and the digits against the
+    reference's golden hash."""
+    import hashlib
+    import fastfib_b200 as ff
+    f = ff.fibonacci(n)
+    t = time.perf_counter()
+    s, done = ff.to_decimal(f)
+    first = (time.perf_counter() - t) * 1e3
+    dev, wall = [], []
+    for _ in range(reps):
+        t = time.perf_counter()
+        s, done = ff.to_decimal(f)
+        wall.append((time.perf_counter() - t) * 1e3)
+        dev.append(ff.last_decimal_ms())
+    with open(os.path.join(ROOT, "tests", "golden", "decimal_sha256.json")) as fh:
+        gold = json.load(fh)
+    ok = bool(done) and str(n) in gold and hashlib.sha256(s.encode()).hexdigest() == gold[str(n)]
+    return {"n": n, "digits": len(s) if s else 0, "device_ms": statistics.median(dev),
+            "e2e_ms": statistics.median(wall), "first_call_ms": first, "device_path": bool(done), "bit_exact": ok}
+
+
 def run_uneven(count=4096, reps=3, seed=4):
     """The uneven product stream: `count` independent products, operand bit
     lengths log-uniform over 2^10..2^24, aspect up to 16:1, uniform random
@@ -312,6 +348,7 @@ def main():
                     help="fib: F(n) (the headline); ntt: one NTT product of --limbs limbs; "
                          "uneven: the uneven product stream, plain against learned dispatch")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-stream figures in the fib line")
+    ap.add_argument("--no-decimal", action="store_true", help="skip the decimal-conversion figures in the fib line")
     ap.add_argument("--limbs", type=int, default=1 << 22)
     ap.add_argument("--square", action="store_true")
     args = ap.parse_args()
@@ -431,6 +468,8 @@ def main():
         }
         if not args.no_uneven and world == 1:
             line["uneven"] = run_uneven(reps=3)
+        if not args.no_decimal and world == 1 and args.n == 10**8:
+            line["decimal"] = run_decimal(args.n)
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.n)
         print(json.dumps(line), flush=True)

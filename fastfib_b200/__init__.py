@@ -109,6 +109,7 @@ def lib() -> ctypes.CDLL:
     L.ffg_get_geometry.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
                                    ctypes.POINTER(ctypes.c_uint32)]
     L.ffg_load_tuning.argtypes = [ctypes.c_char_p]
+    L.ffg_last_decimal_ms.restype = ctypes.c_double
     L.ffg_to_decimal_host.argtypes = [_u64p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p), _szp,
                                       ctypes.POINTER(ctypes.c_int)]
     L.ffg_to_decimal_device.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p), _szp,
@@ -229,6 +230,10 @@ def big_to_string(a) -> str:
     s = ctypes.string_at(p).decode()
     ctypes.CDLL(None).free(ctypes.c_void_p(p))
     return s
+
+
+def last_decimal_ms() -> float:
+    return lib().ffg_last_decimal_ms()
 
 
 def to_decimal(a, device_ptr: int = 0, n: int = 0):

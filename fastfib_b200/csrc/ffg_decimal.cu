@@ -57,10 +57,15 @@ cudaError_t launch_shift_batch(const ShiftJob *d_jobs, uint32_t count, uint64_t 
 
 // ------------------------------------------------------------ combination
 
-constexpr uint32_t COMB_NL = 2048; // limbs per CTA
+constexpr uint32_t COMB_NL = 2048; // most limbs per CTA (a launch uses nl = the pieces' size, 32 .. 2048)
 constexpr uint32_t COMB_THREADS = 256;
 
-__host__ __device__ uint32_t comb_ctas(uint64_t len) { return (uint32_t)((len + COMB_NL - 1) / COMB_NL); }
+__host__ __device__ uint32_t comb_nl(uint64_t max_len) {
+    uint32_t nl = 32;
+    while (nl < COMB_NL && nl < max_len) nl <<= 1;
+    return nl;
+}
+__host__ __device__ uint32_t comb_ctas(uint64_t len, uint32_t nl) { return (uint32_t)((len + nl - 1) / nl); }
 
 struct CombTerms {
     uint64_t mag[3]; // |multiplier| after the device scale
@@ -102,17 +107,17 @@ FFG_DEV_INLINE void comb_colsum(const CombJob &J, const CombTerms &T, uint64_t j
     s_hi = (uint32_t)(acc >> 64);
 }
 
-__global__ void __launch_bounds__(COMB_THREADS) k_comb_batch(const CombJob *__restrict__ jobs) {
+__global__ void __launch_bounds__(COMB_THREADS) k_comb_batch(const CombJob *__restrict__ jobs, uint32_t nl) {
     __shared__ uint64_t lo[COMB_NL];
     __shared__ uint32_t hi[COMB_NL];
     __shared__ uint32_t gG[COMB_NL / 32], gP[COMB_NL / 32], gin[COMB_NL / 32];
     __shared__ uint32_t hiprev_s;
     const CombJob J = jobs[blockIdx.y];
-    const uint32_t ncta = comb_ctas(J.len);
+    const uint32_t ncta = comb_ctas(J.len, nl);
     if (blockIdx.x >= ncta) return;
     const CombTerms T = comb_terms(J);
-    const uint64_t j0 = (uint64_t)blockIdx.x * COMB_NL;
-    for (uint32_t jl = threadIdx.x; jl < COMB_NL; jl += blockDim.x) {
+    const uint64_t j0 = (uint64_t)blockIdx.x * nl;
+    for (uint32_t jl = threadIdx.x; jl < nl; jl += blockDim.x) {
         uint64_t s_lo;
         uint32_t s_hi;
         comb_colsum(J, T, j0 + jl, s_lo, s_hi);
@@ -126,12 +131,12 @@ __global__ void __launch_bounds__(COMB_THREADS) k_comb_batch(const CombJob *__re
         hiprev_s = s_hi;
     }
     __syncthreads();
-    const uint32_t map = cta_resolve(lo, hi, hiprev_s, COMB_NL, gG, gP, gin);
-    for (uint32_t j = threadIdx.x; j < COMB_NL && j0 + j < J.len; j += blockDim.x) J.out[j0 + j] = lo[j];
+    const uint32_t map = cta_resolve(lo, hi, hiprev_s, nl, gG, gP, gin);
+    for (uint32_t j = threadIdx.x; j < nl && j0 + j < J.len; j += blockDim.x) J.out[j0 + j] = lo[j];
     if (threadIdx.x == 0) J.maps[blockIdx.x] = map;
     const bool last = ncta > 1 ? last_cta(J.ticket, ncta) : true;
     if (!last) return;
-    if (ncta > 1) settle_cta(J.out, J.len, COMB_NL, J.maps, ncta);
+    if (ncta > 1) settle_cta(J.out, J.len, nl, J.maps, ncta);
     if (threadIdx.x == 0) {
         uint64_t top = __ldcg(&J.out[J.len - 1]);
         if (J.neg_flag && (top >> 63)) atomicOr(J.neg_flag, 1u);
@@ -143,11 +148,12 @@ __global__ void __launch_bounds__(COMB_THREADS) k_comb_batch(const CombJob *__re
 
 cudaError_t launch_comb_batch(const CombJob *d_jobs, uint32_t count, uint64_t max_len, cudaStream_t st) {
     if (!count) return cudaSuccess;
-    const uint32_t ctas = comb_ctas(max_len);
+    const uint32_t nl = comb_nl(max_len), ctas = comb_ctas(max_len, nl);
+    const uint32_t threads = nl < COMB_THREADS ? nl : COMB_THREADS;
     for (uint32_t base = 0; base < count; base += 65535) {
         const uint32_t cnt = count - base < 65535 ? count - base : 65535;
         prof_begin(PK_LIN, st);
-        k_comb_batch<<<dim3(ctas, cnt), COMB_THREADS, 0, st>>>(d_jobs + base);
+        k_comb_batch<<<dim3(ctas, cnt), threads, 0, st>>>(d_jobs + base, nl);
         prof_end(PK_LIN, st, 32.0 * (double)max_len * cnt);
         cudaError_t e = cudaGetLastError();
         if (e) return e;
@@ -243,6 +249,22 @@ cudaError_t launch_leaf_digits(const LeafJob *d_jobs, uint32_t count, uint32_t c
     prof_begin(PK_LIN, st);
     k_leaf_digits<<<(count + 127) / 128, 128, 0, st>>>(d_jobs, count, chunks, v, d_out);
     prof_end(PK_LIN, st, (double)count * chunks * 19);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------- leading zeros
+
+__global__ void k_first_nonzero(const char *d, uint64_t n, unsigned long long *first) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (d[i] != '0') {
+            atomicMin(first, (unsigned long long)i);
+            return;
+        }
+}
+
+cudaError_t launch_first_nonzero(const char *d, uint64_t n, unsigned long long *d_first, cudaStream_t st) {
+    uint64_t blocks = (n + 255) / 256;
+    k_first_nonzero<<<(uint32_t)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(d, n, d_first);
     return cudaGetLastError();
 }
 

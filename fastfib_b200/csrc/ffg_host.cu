@@ -1950,6 +1950,7 @@ struct DecLevel {
     uint64_t s = 0;                      // bits of P
 };
 static std::vector<DecLevel> g_dec;
+static double g_dec_ms = 0; // device time of the last conversion (levels, leaves, zero scan)
 
 static uint64_t limbs_of(uint64_t bits) { return std::max<uint64_t>(1, (bits + 63) / 64); }
 
@@ -1975,9 +1976,10 @@ static int dev_shift(std::vector<ShiftJob> &jobs, cudaStream_t st) {
 static int dev_comb(std::vector<CombJob> &jobs, cudaStream_t st) {
     if (jobs.empty()) return FFG_OK;
     uint64_t mx = 0;
+    for (auto &j : jobs) mx = std::max(mx, j.len);
+    const uint32_t nl = comb_nl(mx);
     for (auto &j : jobs) {
-        mx = std::max(mx, j.len);
-        j.maps = (uint32_t *)arena_alloc((size_t)comb_ctas(j.len) * 4);
+        j.maps = (uint32_t *)arena_alloc((size_t)comb_ctas(j.len, nl) * 4);
         if (!j.maps) return fail(FFG_E_NOMEM, "device arena: combination maps");
         j.ticket = ticket_get();
     }
@@ -2116,6 +2118,7 @@ static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, s
     }
     CK(cudaStreamSynchronize(st));
     arena_reset();
+    ev_record(g.ev0, st);
     uint32_t *flag = (uint32_t *)arena_alloc(4);
     uint64_t *one = (uint64_t *)arena_alloc(8);
     if (!flag || !one) return fail(FFG_E_NOMEM, "device arena: flag");
@@ -2209,23 +2212,32 @@ static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, s
     const uint64_t v = (uint64_t)((~(u128h)0) / kDec19 - ((u128h)1 << 64));
     cudaError_t e = launch_leaf_digits((const LeafJob *)dl, (uint32_t)lj.size(), chunks, v, dd, st);
     if (e) return fail(FFG_E_CUDA, "decimal leaves: %s", cudaGetErrorString(e));
-    char *h = (char *)malloc(total + 1);
-    if (!h) return fail(FFG_E_NOMEM, "host digits");
+    // leading zeros found on the device; only the digits cross to the host
+    unsigned long long *dfirst = (unsigned long long *)arena_alloc(8);
+    if (!dfirst) return fail(FFG_E_NOMEM, "device arena: digits");
+    const unsigned long long none = total - 1;
+    CK(cudaMemcpyAsync(dfirst, &none, 8, cudaMemcpyHostToDevice, st));
+    if ((e = launch_first_nonzero(dd, total, dfirst, st))) return fail(FFG_E_CUDA, "digits: %s", cudaGetErrorString(e));
+    ev_record(g.ev1, st);
+    unsigned long long first = 0;
     uint32_t hflag = 0;
-    CK(cudaMemcpyAsync(h, dd, total, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&first, dfirst, 8, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, g.ev0, g.ev1) == cudaSuccess) g_dec_ms = ms;
     if (hflag) {
-        free(h);
         *fallback = true;
         return FFG_OK;
     }
-    uint64_t z = 0;
-    while (z + 1 < total && h[z] == '0') z++;
-    memmove(h, h + z, total - z);
-    h[total - z] = 0;
+    const uint64_t nd = total - first;
+    char *h = (char *)malloc(nd + 1);
+    if (!h) return fail(FFG_E_NOMEM, "host digits");
+    CK(cudaMemcpyAsync(h, dd + first, nd, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    h[nd] = 0;
     *out = h;
-    *nout = total - z;
+    *nout = nd;
     return FFG_OK;
 }
 
@@ -2280,3 +2292,5 @@ extern "C" int ffg_to_decimal_host(const uint64_t *x, size_t nx, char **out, siz
     cudaFree(dx);
     return rc;
 }
+
+extern "C" double ffg_last_decimal_ms(void) { return g_dec_ms; }

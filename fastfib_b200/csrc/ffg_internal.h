@@ -159,7 +159,7 @@ struct CombJob {
     uint32_t top_bits;
     uint32_t *neg_flag;         // nullable: raised (atomic or) on a negative result
     uint32_t *sign_out;         // nullable: written 1 / 0 for a negative / non-negative result
-    uint32_t *maps;             // comb_ctas(len) words
+    uint32_t *maps;             // comb_ctas(len, nl) words
     uint32_t *ticket;
 };
 
@@ -180,7 +180,9 @@ struct LeafJob {
     uint64_t n;
 };
 
-__host__ __device__ uint32_t comb_ctas(uint64_t len);
+__host__ __device__ uint32_t comb_nl(uint64_t max_len);           // limbs per CTA of a launch
+__host__ __device__ uint32_t comb_ctas(uint64_t len, uint32_t nl);
+cudaError_t launch_first_nonzero(const char *d, uint64_t n, unsigned long long *d_first, cudaStream_t st);
 cudaError_t launch_shift_batch(const ShiftJob *d_jobs, uint32_t count, uint64_t max_out, cudaStream_t st);
 cudaError_t launch_comb_batch(const CombJob *d_jobs, uint32_t count, uint64_t max_len, cudaStream_t st);
 cudaError_t launch_khat_batch(const KhatJob *d_jobs, uint32_t count, cudaStream_t st);

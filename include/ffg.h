@@ -156,6 +156,9 @@ int ffg_time_batch(ffg_job *jobs, size_t count, int reps, double *ms);
    path). */
 int ffg_to_decimal_device(const uint64_t *x, size_t nx, char **out, size_t *nout, int *done);
 int ffg_to_decimal_host(const uint64_t *x, size_t nx, char **out, size_t *nout, int *done);
+/* Device milliseconds of the last conversion's levels and leaves (CUDA
+   events; the powers, reciprocals and copies excluded). */
+double ffg_last_decimal_ms(void);
 
 /* Tuned four-step geometry for transform length 2^lg (r3 0) or 3 * 2^lg
    (r3 1): rows of 2^row_lg words and column tiles of wc columns (the
