@@ -165,17 +165,24 @@ def run_reference(args, rank, world):
 
 
 def run_ntt_microbench(args):
-    """One NTT product of --limbs random 64-bit limbs (seeded), square or
-    distinct, repeated: per-family device times and the row pass's fraction of
-    the HBM roofline at that length.  Operands stay on the device."""
+    line = ntt_microbench(args.limbs, args.square, args.steps, args.warmup)
+    print(json.dumps(line), flush=True)
+    return 0 if line["bit_exact"] else 1
+
+
+def ntt_microbench(limbs, square, steps, warmup):
+    """One NTT product of `limbs` random 64-bit limbs (seeded), square or
+    distinct, repeated: per-family device times and each pass's fraction of
+    the HBM roofline at that length (8 L bytes per prime per pass, twiddles
+    excluded).  Operands stay on the device; L2 flushed before each step."""
     import numpy as np
     import torch
     import fastfib_b200 as ff
     torch.cuda.set_device(0)
     ff.set_device(0)
-    ff.init(args.limbs * 2)
+    ff.init(limbs * 2)
     rng = np.random.default_rng(88172645463325252 % 2**63)
-    n = args.limbs
+    n = limbs
     a = rng.integers(0, 2**64, n, dtype=np.uint64)
     b = rng.integers(0, 2**64, n, dtype=np.uint64)
     a[-1] |= np.uint64(1 << 63)
@@ -184,18 +191,18 @@ def run_ntt_microbench(args):
     db = torch.from_numpy(b.view(np.int64)).cuda()
     out = torch.zeros(2 * n + 1, dtype=torch.int64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    sq = args.square
+    sq = square
     plan = ff.plan(64 * n, 64 * n, sq)
 
     def step():
         ff.mul_device(out.data_ptr(), da.data_ptr(), n, 64 * n, db.data_ptr(), n, 64 * n, sq)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     ff.profile(True)
     t_ms = []
-    for i in range(args.steps):
+    for i in range(steps):
         flush.fill_(i & 0xFF)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -221,13 +228,17 @@ def run_ntt_microbench(args):
                "gbs": v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else 0.0,
                "frac": (v["bytes"] / (v["ms"] * 1e-3) / 1e9 / peak) if v["ms"] else 0.0}
            for k, v in prof.items() if v["launches"]}
-    line = {"metric": "NTT multiply ms (microbench)", "value": statistics.mean(t_ms), "unit": "ms",
-            "higher_is_better": False, "steps": args.steps, "warmup": args.warmup, "dtype": "u32",
+    passes = [k for k in ("col_fwd", "row_conv", "col_inv") if k in fam]
+    pb = sum(prof[k]["bytes"] for k in passes)
+    pm = sum(prof[k]["ms"] for k in passes)
+    return {"metric": "NTT multiply ms (microbench)", "value": statistics.mean(t_ms), "unit": "ms",
+            "higher_is_better": False, "steps": steps, "warmup": warmup, "dtype": "u32",
             "config": {"workload": f"{'square' if sq else 'product'} of {n}-limb random operands", "plan": plan,
                        "l2": "flushed before every step"},
-            "bit_exact": ok, "families": fam, "peak_gbs": peak}
-    print(json.dumps(line), flush=True)
-    return 0 if ok else 1
+            "bit_exact": ok, "families": fam, "peak_gbs": peak,
+            "ntt_passes": {"gbs": pb / (pm * 1e-3) / 1e9 if pm else 0.0,
+                           "frac": (pb / (pm * 1e-3) / 1e9 / peak) if pm else 0.0,
+                           "of": "measured (MEASURED_PEAKS.json hbm_gbs)"}}
 
 
 def run_decimal(n=10**8, reps=3):
@@ -235,13 +246,15 @@ def run_decimal(n=10**8, reps=3):
     big_to_string, level by level with batched Barrett products): device ms
     of the levels and leaves (powers and reciprocals cached after the first
     call), wall ms of the host API call (number copied in, digits copied
-    out), the first call with the powers, and the digits against the
-    reference's golden hash."""
+    out), one call with the powers and reciprocals recomputed, and the digits
+    against the reference's golden hash."""
     import hashlib
     import fastfib_b200 as ff
     f = ff.fibonacci(n)
+    ff.to_decimal(f)  # the process's first conversion: arena growth, module loading
+    ff.decimal_cache_clear()
     t = time.perf_counter()
-    s, done = ff.to_decimal(f)
+    s, done = ff.to_decimal(f)  # powers and reciprocals recomputed, as the reference does every call
     first = (time.perf_counter() - t) * 1e3
     dev, wall = [], []
     for _ in range(reps):
@@ -253,7 +266,9 @@ def run_decimal(n=10**8, reps=3):
         gold = json.load(fh)
     ok = bool(done) and str(n) in gold and hashlib.sha256(s.encode()).hexdigest() == gold[str(n)]
     return {"n": n, "digits": len(s) if s else 0, "device_ms": statistics.median(dev),
-            "e2e_ms": statistics.median(wall), "first_call_ms": first, "device_path": bool(done), "bit_exact": ok}
+            "e2e_ms": statistics.median(wall), "uncached_e2e_ms": first, "device_path": bool(done), "bit_exact": ok,
+            "note": "device_ms / e2e_ms: powers of ten and reciprocals cached from an earlier call; "
+                    "uncached_e2e_ms: recomputed inside the call, as the reference's big_to_string does"}
 
 
 def run_uneven(count=4096, reps=3, seed=4):
@@ -321,8 +336,9 @@ def run_uneven(count=4096, reps=3, seed=4):
         if any(z % p != (x % p) * (y % p) % p for p in primes) or z.bit_length() > 64 * (a.size + b.size):
             ok = False
             break
-    # end to end through the host API (pinned staging inside the library)
-    ff.mul_batch(pairs[:8], "learned")
+    # end to end through the host API (pinned staging inside the library,
+    # sized by a first full call)
+    ff.mul_batch(pairs, "learned")
     t = time.perf_counter()
     ff.mul_batch(pairs, "learned")
     e2e = (time.perf_counter() - t) * 1e3
@@ -349,6 +365,7 @@ def main():
                          "uneven: the uneven product stream, plain against learned dispatch")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-stream figures in the fib line")
     ap.add_argument("--no-decimal", action="store_true", help="skip the decimal-conversion figures in the fib line")
+    ap.add_argument("--no-ntt", action="store_true", help="skip the L = 2^24 NTT-pass roofline in the fib line")
     ap.add_argument("--limbs", type=int, default=1 << 22)
     ap.add_argument("--square", action="store_true")
     args = ap.parse_args()
@@ -470,6 +487,11 @@ def main():
             line["uneven"] = run_uneven(reps=3)
         if not args.no_decimal and world == 1 and args.n == 10**8:
             line["decimal"] = run_decimal(args.n)
+        if not args.no_ntt and world == 1:
+            nb = ntt_microbench(1 << 22, True, 3, 3)
+            line["ntt_l2e24"] = {"workload": nb["config"]["workload"], "L": nb["config"]["plan"]["L"],
+                                 "ms": nb["value"], "passes": nb["ntt_passes"], "families": nb["families"],
+                                 "bit_exact": nb["bit_exact"]}
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.n)
         print(json.dumps(line), flush=True)

@@ -236,6 +236,10 @@ def last_decimal_ms() -> float:
     return lib().ffg_last_decimal_ms()
 
 
+def decimal_cache_clear() -> None:
+    lib().ffg_decimal_cache_clear()
+
+
 def to_decimal(a, device_ptr: int = 0, n: int = 0):
     """ffg_to_decimal_host (or _device with device_ptr, n limbs): (digits,
     True) from the device path, or (None, False) when it declined."""

@@ -2294,3 +2294,9 @@ extern "C" int ffg_to_decimal_host(const uint64_t *x, size_t nx, char **out, siz
 }
 
 extern "C" double ffg_last_decimal_ms(void) { return g_dec_ms; }
+
+extern "C" void ffg_decimal_cache_clear(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (g.ready) cudaStreamSynchronize(g.stream);
+    dec_free();
+}

@@ -159,6 +159,9 @@ int ffg_to_decimal_host(const uint64_t *x, size_t nx, char **out, size_t *nout, 
 /* Device milliseconds of the last conversion's levels and leaves (CUDA
    events; the powers, reciprocals and copies excluded). */
 double ffg_last_decimal_ms(void);
+/* Drops the powers of ten and reciprocals the conversion keeps on the device
+   between calls (the next conversion recomputes them). */
+void ffg_decimal_cache_clear(void);
 
 /* Tuned four-step geometry for transform length 2^lg (r3 0) or 3 * 2^lg
    (r3 1): rows of 2^row_lg words and column tiles of wc columns (the
