@@ -417,6 +417,7 @@ def main():
     torch.cuda.synchronize()
     barrier()
     with ClockSampler(local) as clk:
+        t_load = time.perf_counter()
         for i in range(args.steps):
             flush.fill_(i & 0xFF)
             torch.cuda.synchronize()
@@ -426,7 +427,13 @@ def main():
             dev_ms.append(ff.last_chain_ms())
         torch.cuda.synchronize()
         barrier()
-    launches = ff.launch_count() - launches0
+        launches = ff.launch_count() - launches0
+        # the timed steps last milliseconds, less than nvidia-smi's sampling
+        # period: the same chain keeps the GPU under load (untimed) until the
+        # sampler has seen it for over a second
+        while time.perf_counter() - t_load < 1.2:
+            ff.fibonacci(args.n)
+        torch.cuda.synchronize()
     h2d, d2h = ff.last_chain_io()
     # the roofline pass: the same K steps again with CUDA events around every
     # launch of the dominant family (events perturb the chain, so `value`

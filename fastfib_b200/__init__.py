@@ -240,6 +240,13 @@ def decimal_cache_clear() -> None:
     lib().ffg_decimal_cache_clear()
 
 
+def tickets_in_use() -> int:
+    """ffg_tickets_in_use: non-zero words of the carry-settle ticket pool (0 when idle)."""
+    f = lib().ffg_tickets_in_use
+    f.restype = ctypes.c_int64
+    return f()
+
+
 def to_decimal(a, device_ptr: int = 0, n: int = 0):
     """ffg_to_decimal_host (or _device with device_ptr, n limbs): (digits,
     True) from the device path, or (None, False) when it declined."""

@@ -136,7 +136,10 @@ __global__ void __launch_bounds__(COMB_THREADS) k_comb_batch(const CombJob *__re
     if (threadIdx.x == 0) J.maps[blockIdx.x] = map;
     const bool last = ncta > 1 ? last_cta(J.ticket, ncta) : true;
     if (!last) return;
-    if (ncta > 1) settle_cta(J.out, J.len, nl, J.maps, ncta);
+    // thread 0 reads and may rewrite the top limb: every store of the CTA
+    // (its own limbs, the settled carries) must be done first
+    if (ncta > 1) settle_cta(J.out, J.len, nl, J.maps, ncta); // ends with a barrier
+    else __syncthreads();
     if (threadIdx.x == 0) {
         uint64_t top = __ldcg(&J.out[J.len - 1]);
         if (J.neg_flag && (top >> 63)) atomicOr(J.neg_flag, 1u);

@@ -2119,10 +2119,11 @@ static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, s
     CK(cudaStreamSynchronize(st));
     arena_reset();
     ev_record(g.ev0, st);
-    uint32_t *flag = (uint32_t *)arena_alloc(4);
+    // flags per level: [2 l] estimate out of range, [2 l + 1] negative remainder
+    uint32_t *flags = (uint32_t *)arena_alloc(8 * (T + 1));
     uint64_t *one = (uint64_t *)arena_alloc(8);
-    if (!flag || !one) return fail(FFG_E_NOMEM, "device arena: flag");
-    CK(cudaMemsetAsync(flag, 0, 4, st));
+    if (!flags || !one) return fail(FFG_E_NOMEM, "device arena: flag");
+    CK(cudaMemsetAsync(flags, 0, 8 * (T + 1), st));
     const uint64_t h_one = 1;
     CK(cudaMemcpyAsync(one, &h_one, 8, cudaMemcpyHostToDevice, st));
     // pieces of the current level: pointer, limbs, bit bound
@@ -2159,7 +2160,7 @@ static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, s
         if ((rc = dev_products(pr, st))) return rc;
         std::vector<KhatJob> kj;
         for (uint64_t p = 0; p < cnt; p++)
-            kj.push_back(KhatJob{cur[p].d, qp + p * nqp, L.P, cur[p].n, nqp, L.nP, s, kh + p, flag});
+            kj.push_back(KhatJob{cur[p].d, qp + p * nqp, L.P, cur[p].n, nqp, L.nP, s, kh + p, flags + 2 * l});
         void *dk;
         if ((rc = dev_upload_jobs(kj.data(), kj.size() * sizeof(KhatJob), &dk, st))) return rc;
         cudaError_t e = launch_khat_batch((const KhatJob *)dk, (uint32_t)cnt, st);
@@ -2181,7 +2182,7 @@ static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, s
             CombJob c{}; // r = r1 + sign P
             c.src[0] = r1 + p * nr, c.n[0] = nr, c.mul[0] = 1;
             c.src[1] = L.P, c.n[1] = std::min(L.nP, nr), c.mul[1] = 1, c.scale[1] = sg + p;
-            c.out = r + p * nr, c.len = nr, c.neg_flag = flag;
+            c.out = r + p * nr, c.len = nr, c.neg_flag = flags + 2 * l + 1;
             cj.push_back(c);
             CombJob d{}; // q + k - sign
             d.src[0] = q + p * nq, d.n[0] = nq, d.mul[0] = 1, d.add_dev = kh + p;
@@ -2220,16 +2221,20 @@ static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, s
     if ((e = launch_first_nonzero(dd, total, dfirst, st))) return fail(FFG_E_CUDA, "digits: %s", cudaGetErrorString(e));
     ev_record(g.ev1, st);
     unsigned long long first = 0;
-    uint32_t hflag = 0;
+    std::vector<uint32_t> hflags(2 * (T + 1));
     CK(cudaMemcpyAsync(&first, dfirst, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hflags.data(), flags, 8 * (T + 1), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     float ms = 0;
     if (cudaEventElapsedTime(&ms, g.ev0, g.ev1) == cudaSuccess) g_dec_ms = ms;
-    if (hflag) {
-        *fallback = true;
-        return FFG_OK;
-    }
+    for (int l = 0; l <= T; l++)
+        if (hflags[2 * l] || hflags[2 * l + 1]) {
+            // not an error: the caller converts another way; the reason stays readable
+            g.err = "decimal conversion declined at level " + std::to_string(l) +
+                    (hflags[2 * l] ? ": quotient estimate out of range" : ": negative remainder");
+            *fallback = true;
+            return FFG_OK;
+        }
     const uint64_t nd = total - first;
     char *h = (char *)malloc(nd + 1);
     if (!h) return fail(FFG_E_NOMEM, "host digits");
@@ -2299,4 +2304,17 @@ extern "C" void ffg_decimal_cache_clear(void) {
     std::lock_guard<std::recursive_mutex> lk(g_mu);
     if (g.ready) cudaStreamSynchronize(g.stream);
     dec_free();
+}
+
+// Words of the ticket pool that are not zero (all must be, between calls).
+extern "C" int64_t ffg_tickets_in_use(void) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    if (!g_tickets) return 0;
+    cudaStreamSynchronize(g.stream);
+    const size_t nt = (size_t)kTicketsLive + kTicketsCapture + 1;
+    std::vector<uint32_t> h(nt);
+    if (cudaMemcpy(h.data(), g_tickets, nt * 4, cudaMemcpyDeviceToHost)) return -1;
+    int64_t c = 0;
+    for (uint32_t v : h) c += v != 0;
+    return c;
 }

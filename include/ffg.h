@@ -163,6 +163,10 @@ double ffg_last_decimal_ms(void);
    between calls (the next conversion recomputes them). */
 void ffg_decimal_cache_clear(void);
 
+/* Words of the in-launch carry-settle ticket pool that are not zero (0 when
+   the GPU is idle; a diagnostic). */
+int64_t ffg_tickets_in_use(void);
+
 /* Tuned four-step geometry for transform length 2^lg (r3 0) or 3 * 2^lg
    (r3 1): rows of 2^row_lg words and column tiles of wc columns (the
    reference's fixed pass shapes, src/ntt_conv.c:158-226, have no tuned

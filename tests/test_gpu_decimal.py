@@ -21,7 +21,7 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "decim
 
 def device_digits(ff, x):
     s, done = ff.to_decimal(int_to_limbs(x) if isinstance(x, int) else x)
-    assert done, "the device path declined"
+    assert done, "the device path declined: " + ff.lib().ffg_last_error().decode()
     return s
 
 
@@ -63,3 +63,18 @@ def test_device_pointer_entry(ff):
     t = torch.from_numpy(a.view(np.int64)).cuda()
     s, done = ff.to_decimal(None, device_ptr=t.data_ptr(), n=a.size)
     assert done and s == str(x)
+
+
+def test_after_other_work(ff):
+    """The arena is reused across calls: a conversion after a large batch of
+    products (its buffers full of other data) must still be exact, and every
+    ticket of the in-launch carry settle must be back at zero."""
+    from fastfib_b200.workload import uneven_products
+    with open(GOLD) as f:
+        gold = json.load(f)
+    x = ff.fibonacci(10**7)
+    assert hashlib.sha256(device_digits(ff, x).encode()).hexdigest() == gold["10000000"]
+    ff.mul_batch(uneven_products(seed=9, count=1500, lo=12, hi=23), "plain")
+    for _ in range(2):
+        assert hashlib.sha256(device_digits(ff, x).encode()).hexdigest() == gold["10000000"]
+    assert ff.tickets_in_use() == 0
