@@ -43,6 +43,17 @@ FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t ct
 
 __global__ void __launch_bounds__(CRT_THREADS) k_crt(GarnerConst K, CrtJob J) { crt_block(K, J, blockIdx.x); }
 
+// Up to two CRTs by value (the doubling step's two squarings): product
+// blockIdx.y, its CTA blockIdx.x.
+struct CrtPair {
+    CrtJob j[2];
+};
+__global__ void __launch_bounds__(CRT_THREADS) k_crt_pair(GarnerConst K, CrtPair P) {
+    const CrtJob &J = P.j[blockIdx.y];
+    if (blockIdx.x >= crt_ctas_dev(J.nlimbs, J.width)) return;
+    crt_block(K, J, blockIdx.x);
+}
+
 // A batch of CRTs: product blockIdx.y, its CTA blockIdx.x (CTAs past the
 // product's own count return at once, all threads together).
 __global__ void __launch_bounds__(CRT_THREADS) k_crt_batch(GarnerConst K, const CrtJob *__restrict__ jobs) {
@@ -167,6 +178,26 @@ cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st) {
     prof_begin(PK_CRT, st);
     k_crt<<<ncta, CRT_THREADS, crt_smem(), st>>>(garner_const(), J);
     prof_end(PK_CRT, st, 12.0 * (double)J.conv + 8.0 * (double)J.nlimbs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt_pair(const CrtJob *jobs, uint32_t count, cudaStream_t st) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_crt_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)crt_smem());
+        if (e) return e;
+        configured = true;
+    }
+    if (count == 1) return launch_crt(Primes3{}, jobs[0], st);
+    CrtPair P;
+    P.j[0] = jobs[0];
+    P.j[1] = jobs[1];
+    const uint32_t n0 = crt_ctas(jobs[0].nlimbs, jobs[0].width), n1 = crt_ctas(jobs[1].nlimbs, jobs[1].width);
+    double bytes = 0;
+    for (int i = 0; i < 2; i++) bytes += 12.0 * (double)jobs[i].conv + 8.0 * (double)jobs[i].nlimbs;
+    prof_begin(PK_CRT, st);
+    k_crt_pair<<<dim3(n0 > n1 ? n0 : n1, 2), CRT_THREADS, crt_smem(), st>>>(garner_const(), P);
+    prof_end(PK_CRT, st, bytes);
     return cudaGetLastError();
 }
 

@@ -571,8 +571,10 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
         e = launch_four_step(g.P3, G, jobs, (uint32_t)count, st, limb_bytes);
         if (e) return fail(FFG_E_CUDA, "four_step: %s", cudaGetErrorString(e));
     }
+    CrtJob crt[FFG_FS_JOBS];
     for (int i = 0; i < count; i++) {
-        CrtJob C{};
+        CrtJob &C = crt[i];
+        C = CrtJob{};
         C.y = ya[i];
         C.y_stride = L;
         uint64_t ca = (pr[i].bits_a + w - 1) / w, cb = square ? ca : (pr[i].bits_b + w - 1) / w;
@@ -584,7 +586,9 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
         C.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(C.nlimbs, w) * sizeof(uint32_t));
         if (!C.maps) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
         C.ticket = ticket_get();
-        e = launch_crt(g.P3, C, st);
+    }
+    for (int i = 0; i < count; i += 2) { // the step's pair in one launch
+        e = launch_crt_pair(crt + i, count - i >= 2 ? 2 : 1, st);
         if (e) return fail(FFG_E_CUDA, "crt: %s", cudaGetErrorString(e));
     }
     return FFG_OK;
@@ -1941,7 +1945,12 @@ extern "C" int ffg_load_tuning(const char *path) {
 
 namespace ffg {
 
-static const int kDecLeafLg = 4; // DEC_LEAF_LG (src/decimal.c): leaves below 10^(19 * 32)
+// Leaves: pieces below 10^(19 2^(kDecLeafLg + 1)) = 10^2432 (at most 128 limbs),
+// one thread each.  The reference stops its recursion two levels lower
+// (DEC_LEAF_LG = 4, src/decimal.c); here the two lowest levels would hold tens
+// of thousands of pieces whose job records cost more host time than their
+// arithmetic costs the GPU.
+static const int kDecLeafLg = 6;
 static const uint64_t kDec19 = 10000000000000000000ull;
 
 struct DecLevel {
@@ -1990,12 +1999,23 @@ static int dev_comb(std::vector<CombJob> &jobs, cudaStream_t st) {
     return e ? fail(FFG_E_CUDA, "decimal combination: %s", cudaGetErrorString(e)) : FFG_OK;
 }
 
-// Products out_i = a_i b_i (out_i: na + nb + 1 limbs), the plain thresholds.
+// Products out_i = a_i b_i (out_i: na + nb + 1 limbs), the plain thresholds
+// (a level's products share one shape: the plan is looked up once a shape).
 static int dev_products(std::vector<BJob> &jobs, cudaStream_t st) {
     std::vector<BJob> run;
+    run.reserve(jobs.size());
+    BJob last{};
+    bool have = false;
     for (BJob J : jobs) {
-        const int rc = method_plan(FFG_M_PLAIN, J.bits_a, J.bits_b, J.square, &J);
-        if (rc) return rc;
+        if (have && J.bits_a == last.bits_a && J.bits_b == last.bits_b && J.square == last.square) {
+            J.school = last.school;
+            J.pl = last.pl;
+        } else {
+            const int rc = method_plan(FFG_M_PLAIN, J.bits_a, J.bits_b, J.square, &J);
+            if (rc) return rc;
+            last = J;
+            have = true;
+        }
         run.push_back(J);
     }
     return run_batch(run, st);

@@ -174,7 +174,7 @@ struct KhatJob {
 };
 
 // One leaf piece (below 10^(19 chunks)).
-constexpr int FFG_LEAF_MAX_LIMBS = 34;
+constexpr int FFG_LEAF_MAX_LIMBS = 130;
 struct LeafJob {
     const uint64_t *x;
     uint64_t n;
@@ -208,6 +208,7 @@ cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJobs &jo
                                  cudaStream_t st, double limb_bytes);
 cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob &job, uint32_t pairs, cudaStream_t st);
 cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st);
+cudaError_t launch_crt_pair(const CrtJob *jobs, uint32_t count, cudaStream_t st); // count 1 or 2, by value
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st);
 
 // The cost model's kernels (ffg_mlp.cu); parameters, rows and outputs on the device.

@@ -151,7 +151,8 @@ int ffg_time_batch(ffg_job *jobs, size_t count, int reps, double *ms);
    the device level by level: every level's Barrett products in shared
    launches.  *out is a malloc'd NUL-terminated string of *nout digits (free
    with free()).  *done = 0 when the device path declines -- numbers below
-   about 10^1200 and the rare case of a quotient correction out of range --
+   about 10^4900 and a quotient correction out of range (which its bounds
+   rule out) --
    and the caller converts another way (big_to_string then uses its host
    path). */
 int ffg_to_decimal_device(const uint64_t *x, size_t nx, char **out, size_t *nout, int *done);
