@@ -248,7 +248,26 @@ FFG_DEV_INLINE void school_col(const SchoolJob &J, int64_t j, uint64_t &t0, uint
     }
 }
 
+FFG_DEV_INLINE void school_block(const SchoolJob &J);
+
 __global__ void __launch_bounds__(SCHOOL_THREADS) k_school(const SchoolJob *__restrict__ jobs) {
+    const SchoolJob J = jobs[blockIdx.y];
+    if (blockIdx.x >= school_ctas(J.nlimbs)) return;
+    school_block(J);
+}
+
+// Up to two schoolbook products by value (the doubling step's two squarings
+// while the operands are short).
+struct SchoolPair {
+    SchoolJob j[2];
+};
+__global__ void __launch_bounds__(SCHOOL_THREADS) k_school_pair(SchoolPair P) {
+    const SchoolJob &J = P.j[blockIdx.y];
+    if (blockIdx.x >= school_ctas(J.nlimbs)) return;
+    school_block(J);
+}
+
+FFG_DEV_INLINE void school_block(const SchoolJob &J) {
     constexpr uint32_t NC = SCHOOL_NL + 3; // columns j0 - 3 .. j0 + NL - 1
     __shared__ uint64_t t0s[NC], t1s[NC];
     __shared__ uint32_t t2s[NC];
@@ -256,8 +275,6 @@ __global__ void __launch_bounds__(SCHOOL_THREADS) k_school(const SchoolJob *__re
     __shared__ uint32_t hi[SCHOOL_NL];
     __shared__ uint32_t gG[SCHOOL_NL / 32], gP[SCHOOL_NL / 32], gin[SCHOOL_NL / 32];
     __shared__ uint32_t hiprev_s;
-    const SchoolJob J = jobs[blockIdx.y];
-    if (blockIdx.x >= school_ctas(J.nlimbs)) return;
     const int64_t j0 = (int64_t)blockIdx.x * SCHOOL_NL;
     for (uint32_t c = threadIdx.x; c < NC; c += blockDim.x) {
         uint64_t a, b, d;
@@ -286,6 +303,21 @@ __global__ void __launch_bounds__(SCHOOL_THREADS) k_school(const SchoolJob *__re
         settle_cta(J.out, J.nlimbs, SCHOOL_NL, J.maps, ncta);
         if (threadIdx.x == 0) *J.ticket = 0;
     }
+}
+
+cudaError_t launch_school_pair(const SchoolJob *jobs, uint32_t count, cudaStream_t st) {
+    SchoolPair P{};
+    uint32_t mx = 0;
+    double bytes = 0;
+    for (uint32_t i = 0; i < count && i < 2; i++) {
+        P.j[i] = jobs[i];
+        mx = max(mx, school_ctas(jobs[i].nlimbs));
+        bytes += 8.0 * (double)(jobs[i].na + jobs[i].nb + jobs[i].nlimbs);
+    }
+    prof_begin(PK_SCHOOL, st);
+    k_school_pair<<<dim3(mx, count), SCHOOL_THREADS, 0, st>>>(P);
+    prof_end(PK_SCHOOL, st, bytes);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,

@@ -25,6 +25,10 @@ static const uint32_t kG[3] = {5u, 31u, 13u};
 static int kMaxLg = 25; // NTT_MAX_LG (src/common.h:46-48); ffg_set_max_lg lowers it like -DNTT_MAX_LG
 static const uint32_t kSmallMaxL = 4096;  // one-CTA transform up to this length for a single product
 static const int kR3TabLg = 13;           // radix-3 tables cover R = 3 2^n, n < 13
+// Doubling steps whose operands have at most this many limbs square by
+// schoolbook (one launch for the pair) instead of the NTT (transform + CRT):
+// at these sizes both are latency-bound and the schoolbook takes one launch.
+static const uint64_t kChainSchoolLimbs = 256;
 
 // ------------------------------------------------------------ host modmath
 
@@ -746,7 +750,24 @@ static int chain_body(uint64_t n, int i0, uint64_t *fk, uint64_t *fkm1, uint64_t
         int rc = plan_select(bk, bk, 1, &pl1);
         if (!rc) rc = plan_select(bkm1, bkm1, 1, &pl2);
         if (rc) return rc;
-        if (pl1.split || pl2.split) {
+        if (nk <= kChainSchoolLimbs) {
+            // short operands: both squarings as schoolbook products, one launch
+            SchoolJob sj[2];
+            const Prod *pp[2] = {&p1, &p2};
+            for (int q = 0; q < 2; q++) {
+                SchoolJob &J = sj[q];
+                J = SchoolJob{};
+                J.a = J.b = pp[q]->a;
+                J.na = J.nb = (pp[q]->bits_a + 63) / 64;
+                J.out = pp[q]->out;
+                J.nlimbs = 2 * pp[q]->na + 1;
+                J.maps = (uint32_t *)arena_alloc((size_t)school_ctas(J.nlimbs) * 4);
+                if (!J.maps) return fail(FFG_E_NOMEM, "device arena: schoolbook maps");
+                J.ticket = ticket_get();
+            }
+            cudaError_t e = launch_school_pair(sj, 2, st);
+            if (e) return fail(FFG_E_CUDA, "schoolbook pair: %s", cudaGetErrorString(e));
+        } else if (pl1.split || pl2.split) {
             rc = mul_one(p1, true, st);
             if (!rc) rc = mul_one(p2, true, st);
         } else if (pl1.width == pl2.width && pl1.L == pl2.L && pl1.kernel == pl2.kernel &&
