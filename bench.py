@@ -241,6 +241,19 @@ def ntt_microbench(limbs, square, steps, warmup):
                            "of": "measured (MEASURED_PEAKS.json hbm_gbs)"}}
 
 
+def job_ms(totals, steps, world, device="cuda"):
+    """Replicas: each of `world` ranks ran `steps` chains in totals = [device
+    ms, host ms]; the job's time is the max over ranks (an all-reduce MAX when
+    world > 1), and per F(n) of the whole job it is that over steps * world."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor(list(totals), dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        totals = t.tolist()
+    return [v / (steps * world) for v in totals]
+
+
 def run_decimal(n=10**8, reps=3):
     """Decimal digits of F(n) through the device conversion (the reference's
     big_to_string, level by level with batched Barrett products): device ms
@@ -449,14 +462,7 @@ def main():
     prof = ff.profile_read()[dominant]
     ff.profile(False)
 
-    total_dev = sum(dev_ms)
-    total_e2e = sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([total_dev, total_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_dev, total_e2e = t.tolist()
-    value = total_dev / (args.steps * world)
-    e2e = total_e2e / (args.steps * world)
+    value, e2e = job_ms([sum(dev_ms), sum(e2e_ms)], args.steps, world)
 
     extra = {}
     if rank == 0 and args.n == 10**8 and world == 1 and not args.no_f1e9:
