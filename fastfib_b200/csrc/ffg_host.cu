@@ -1713,7 +1713,18 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
     uint64_t *din = (uint64_t *)arena_alloc(std::max<uint64_t>(1, in_limbs) * 8);
     uint64_t *dout = (uint64_t *)arena_alloc(std::max<uint64_t>(1, out_limbs) * 8);
     if (!din || !dout) return fail(FFG_E_NOMEM, "device arena: batch operands");
-    uint64_t *hin = (uint64_t *)pinned_get(std::max<uint64_t>(1, in_limbs) * 8);
+    // staging buffers go back to the pool on every path, after the stream is idle
+    struct Staging {
+        void *p = nullptr;
+        cudaStream_t st;
+        ~Staging() {
+            if (p) {
+                cudaStreamSynchronize(st);
+                pinned_release(p);
+            }
+        }
+    } in_buf{nullptr, st}, out_buf{nullptr, st};
+    uint64_t *hin = (uint64_t *)(in_buf.p = pinned_get(std::max<uint64_t>(1, in_limbs) * 8));
     if (!hin) return fail(FFG_E_NOMEM, "pinned staging");
     for (size_t i = 0; i < count; i++) {
         memcpy(hin + aoff[i], jobs[i].a, std::min(na[i], jobs[i].na) * 8);
@@ -1726,11 +1737,7 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
     CK(cudaMemcpyAsync(din, hin, in_limbs * 8, cudaMemcpyHostToDevice, st));
     std::vector<int> sqv(count), meth(count);
     for (size_t i = 0; i < count; i++) sqv[i] = jobs[i].square != 0, meth[i] = jobs[i].method;
-    rc = learned_resolve(ba.data(), bb.data(), sqv.data(), meth.data(), count, st);
-    if (rc) {
-        pinned_release(hin);
-        return rc;
-    }
+    if ((rc = learned_resolve(ba.data(), bb.data(), sqv.data(), meth.data(), count, st))) return rc;
     std::vector<BJob> bj;
     for (size_t i = 0; i < count; i++) {
         if (ba[i] == 0 || bb[i] == 0) {
@@ -1738,37 +1745,20 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
             continue;
         }
         BJob J{din + aoff[i], din + boff[i], na[i], nb[i], ba[i], bb[i], dout + roff[i], jobs[i].square != 0, 0, {}};
-        rc = method_plan(meth[i], ba[i], bb[i], jobs[i].square != 0, &J);
-        if (rc) {
-            pinned_release(hin);
-            return rc;
-        }
+        if ((rc = method_plan(meth[i], ba[i], bb[i], jobs[i].square != 0, &J))) return rc;
         bj.push_back(J);
     }
-    rc = run_batch(bj, st);
-    if (rc) {
-        cudaStreamSynchronize(st);
-        pinned_release(hin);
-        return rc;
-    }
-    uint64_t *hout = (uint64_t *)pinned_get(std::max<uint64_t>(1, out_limbs) * 8);
-    if (!hout) {
-        cudaStreamSynchronize(st);
-        pinned_release(hin);
-        return fail(FFG_E_NOMEM, "pinned staging");
-    }
+    if ((rc = run_batch(bj, st))) return rc;
+    uint64_t *hout = (uint64_t *)(out_buf.p = pinned_get(std::max<uint64_t>(1, out_limbs) * 8));
+    if (!hout) return fail(FFG_E_NOMEM, "pinned staging");
     CK(cudaMemcpyAsync(hout, dout, out_limbs * 8, cudaMemcpyDeviceToHost, st));
-    cudaError_t e = cudaStreamSynchronize(st);
-    if (!e)
-        for (size_t i = 0; i < count; i++) {
-            uint64_t n = na[i] + nb[i];
-            while (n > 1 && hout[roff[i] + n - 1] == 0) n--;
-            memcpy(jobs[i].out, hout + roff[i], n * 8);
-            jobs[i].nout = n;
-        }
-    pinned_release(hin);
-    pinned_release(hout);
-    if (e) return fail(FFG_E_CUDA, "batch: %s", cudaGetErrorString(e));
+    CK(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < count; i++) {
+        uint64_t n = na[i] + nb[i];
+        while (n > 1 && hout[roff[i] + n - 1] == 0) n--;
+        memcpy(jobs[i].out, hout + roff[i], n * 8);
+        jobs[i].nout = n;
+    }
     return FFG_OK;
 }
 
@@ -2091,6 +2081,40 @@ static void dec_free() {
     g_dec.clear();
 }
 
+// Level l (> 0) of the cache from level l - 1: P_l = P_(l-1)^2 with its exact
+// bit length, then m_l from (m_(l-1))^2 and two Newton steps.
+static int dec_level(int l, cudaStream_t st) {
+    DecLevel &L = g_dec[l];
+    const DecLevel &B = g_dec[l - 1];
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    const uint64_t nsq = 2 * B.nP + 1;
+    CK(cudaMalloc(&L.P, nsq * 8));
+    std::vector<BJob> sq{bjob(B.P, B.nP, B.s, nullptr, 0, 0, L.P, true)};
+    int rc = dev_products(sq, st);
+    if (rc) return rc;
+    uint64_t *dbits = (uint64_t *)arena_alloc(8);
+    if (!dbits) return fail(FFG_E_NOMEM, "device arena: bit length");
+    cudaError_t e = launch_bit_length(L.P, nsq, dbits, st);
+    if (e) return fail(FFG_E_CUDA, "decimal powers: %s", cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(&L.s, dbits, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    L.nP = limbs_of(L.s);
+    L.nm = limbs_of(L.s + 1);
+    CK(cudaMalloc(&L.m, L.nm * 8));
+    uint64_t *sqm = (uint64_t *)arena_alloc((2 * B.nm + 1) * 8);
+    uint64_t *y0 = (uint64_t *)arena_alloc(L.nm * 8), *y1 = (uint64_t *)arena_alloc(L.nm * 8);
+    if (!sqm || !y0 || !y1) return fail(FFG_E_NOMEM, "device arena: reciprocal");
+    std::vector<BJob> msq{bjob(B.m, B.nm, B.s + 1, nullptr, 0, 0, sqm, true)};
+    if ((rc = dev_products(msq, st))) return rc;
+    std::vector<ShiftJob> sh{ShiftJob{sqm, 2 * B.nm + 1, y0, L.nm, 4 * B.s - 2 * L.s}};
+    if ((rc = dev_shift(sh, st))) return rc;
+    if ((rc = newton_step(L, y0, L.nm, y1, st))) return rc;
+    if ((rc = newton_step(L, y1, L.nm, L.m, st))) return rc;
+    CK(cudaStreamSynchronize(st));
+    return FFG_OK;
+}
+
 // Levels 0..T of powers and reciprocals (kept between calls).
 static int dec_prepare(int T, cudaStream_t st) {
     while ((int)g_dec.size() <= T) {
@@ -2106,36 +2130,15 @@ static int dec_prepare(int T, cudaStream_t st) {
             g_dec.push_back(L);
             continue;
         }
-        const DecLevel &B = g_dec[l - 1];
-        CK(cudaStreamSynchronize(st));
-        arena_reset();
-        const uint64_t nsq = 2 * B.nP + 1;
-        CK(cudaMalloc(&L.P, nsq * 8));
-        std::vector<BJob> sq{bjob(B.P, B.nP, B.s, nullptr, 0, 0, L.P, true)};
-        int rc = dev_products(sq, st);
-        if (rc) return rc;
-        uint64_t *dbits = (uint64_t *)arena_alloc(8);
-        if (!dbits) return fail(FFG_E_NOMEM, "device arena: bit length");
-        cudaError_t e = launch_bit_length(L.P, nsq, dbits, st);
-        if (e) return fail(FFG_E_CUDA, "decimal powers: %s", cudaGetErrorString(e));
-        CK(cudaMemcpyAsync(&L.s, dbits, 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        L.nP = limbs_of(L.s);
-        // m: start from the previous level's reciprocal squared, two Newton steps
-        L.nm = limbs_of(L.s + 1);
-        CK(cudaMalloc(&L.m, L.nm * 8));
-        uint64_t *sqm = (uint64_t *)arena_alloc((2 * B.nm + 1) * 8);
-        uint64_t *y0 = (uint64_t *)arena_alloc(L.nm * 8), *y1 = (uint64_t *)arena_alloc(L.nm * 8);
-        if (!sqm || !y0 || !y1) return fail(FFG_E_NOMEM, "device arena: reciprocal");
-        std::vector<BJob> msq{bjob(B.m, B.nm, B.s + 1, nullptr, 0, 0, sqm, true)};
-        if ((rc = dev_products(msq, st))) return rc;
-        std::vector<ShiftJob> sh{ShiftJob{sqm, 2 * B.nm + 1, y0, L.nm, 4 * B.s - 2 * L.s}};
-        if ((rc = dev_shift(sh, st))) return rc;
-        g_dec.push_back(L); // newton_step reads P and s through it
-        DecLevel &N = g_dec.back();
-        if ((rc = newton_step(N, y0, N.nm, y1, st))) return rc;
-        if ((rc = newton_step(N, y1, N.nm, N.m, st))) return rc;
-        CK(cudaStreamSynchronize(st));
+        g_dec.push_back(DecLevel{});
+        const int rc = dec_level(l, st);
+        if (rc) { // a level left incomplete is not kept
+            cudaStreamSynchronize(st);
+            if (g_dec.back().P) cudaFree(g_dec.back().P);
+            if (g_dec.back().m) cudaFree(g_dec.back().m);
+            g_dec.pop_back();
+            return rc;
+        }
     }
     return FFG_OK;
 }
