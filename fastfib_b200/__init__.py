@@ -240,6 +240,21 @@ def decimal_cache_clear() -> None:
     lib().ffg_decimal_cache_clear()
 
 
+FP_PRIMES = (18446744073709551557, 18446744073709551533, 9223372036854775783, 4611686018427387847)
+
+
+def fingerprint(a=None, device_ptr: int = 0, n: int = 0) -> list:
+    """ffg_fingerprint_host / _device: [bits, low 64 bits, x mod each of
+    FP_PRIMES], computed on the GPU."""
+    out = (ctypes.c_uint64 * 6)()
+    if device_ptr:
+        _check(lib().ffg_fingerprint_device(ctypes.cast(device_ptr, _u64p), n, out))
+    else:
+        a = _arr(a)
+        _check(lib().ffg_fingerprint_host(a.ctypes.data_as(_u64p), a.size, out))
+    return [int(v) for v in out]
+
+
 def tickets_in_use() -> int:
     """ffg_tickets_in_use: non-zero words of the carry-settle ticket pool (0 when idle)."""
     f = lib().ffg_tickets_in_use

@@ -2362,3 +2362,51 @@ extern "C" int64_t ffg_tickets_in_use(void) {
     for (uint32_t v : h) c += v != 0;
     return c;
 }
+
+// ------------------------------------------------------------ fingerprints
+
+static const uint64_t kFpPrimes[FFG_FP_PRIMES] = {18446744073709551557ull, 18446744073709551533ull,
+                                                  9223372036854775783ull, 4611686018427387847ull};
+
+// The fingerprint of x (device, n limbs) on stream st, scratch from the arena.
+static int fingerprint_dev(const uint64_t *x, size_t n, uint64_t *out, cudaStream_t st) {
+    uint64_t *partial = (uint64_t *)arena_alloc((size_t)fingerprint_blocks() * FFG_FP_PRIMES * 8);
+    uint64_t *res = (uint64_t *)arena_alloc(8 * (FFG_FP_PRIMES + 2));
+    if (!partial || !res) return fail(FFG_E_NOMEM, "device arena: fingerprint");
+    unsigned long long *dbits = (unsigned long long *)(res + FFG_FP_PRIMES);
+    CK(cudaMemsetAsync(dbits, 0, 8, st));
+    cudaError_t e = launch_bits_mb(x, n, dbits, st);
+    if (!e) e = launch_fingerprint(x, n, kFpPrimes, partial, ticket_get(), res, st);
+    if (e) return fail(FFG_E_CUDA, "fingerprint: %s", cudaGetErrorString(e));
+    uint64_t h[FFG_FP_PRIMES + 1], low = 0;
+    CK(cudaMemcpyAsync(h, res, 8 * (FFG_FP_PRIMES + 1), cudaMemcpyDeviceToHost, st));
+    if (n) CK(cudaMemcpyAsync(&low, x, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    out[0] = h[FFG_FP_PRIMES];
+    out[1] = low;
+    for (int k = 0; k < FFG_FP_PRIMES; k++) out[2 + k] = h[k];
+    return FFG_OK;
+}
+
+extern "C" int ffg_fingerprint_device(const uint64_t *x, size_t n, uint64_t *out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if ((!x && n) || !out) return fail(FFG_E_ARG, "ffg_fingerprint_device arguments");
+    CK(cudaStreamSynchronize(g.stream));
+    arena_reset();
+    return fingerprint_dev(x, n, out, g.stream);
+}
+
+extern "C" int ffg_fingerprint_host(const uint64_t *x, size_t n, uint64_t *out) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if ((!x && n) || !out) return fail(FFG_E_ARG, "ffg_fingerprint_host arguments");
+    CK(cudaStreamSynchronize(g.stream));
+    arena_reset();
+    uint64_t *dx = (uint64_t *)arena_alloc(std::max<size_t>(1, n) * 8);
+    if (!dx) return fail(FFG_E_NOMEM, "device arena: fingerprint input");
+    if (n) CK(cudaMemcpyAsync(dx, x, n * 8, cudaMemcpyHostToDevice, g.stream));
+    return fingerprint_dev(dx, n, out, g.stream);
+}

@@ -219,6 +219,13 @@ cudaError_t launch_mlp_grad(const float *d_params, const float *d_X, const int32
                             float *d_grad, float *d_loss, cudaStream_t st);
 cudaError_t launch_mlp_infer(const float *d_params, const float *d_X, uint32_t n, float *d_out, cudaStream_t st);
 
+// Fingerprints (ffg_fingerprint.cu): x mod each prime into d_out, using
+// fingerprint_blocks() * FFG_FP_PRIMES words of partial sums and a zero ticket.
+cudaError_t launch_fingerprint(const uint64_t *x, uint64_t n, const uint64_t *primes, uint64_t *partial,
+                               uint32_t *ticket, uint64_t *d_out, cudaStream_t st);
+uint32_t fingerprint_blocks();
+cudaError_t launch_bits_mb(const uint64_t *x, uint64_t n, unsigned long long *d_out, cudaStream_t st);
+
 // Kernel families the profiler tracks (ffg_profile_read in include/ffg.h).
 enum ProfKind { PK_CONV_SMALL = 0, PK_COL_FWD, PK_ROW_CONV, PK_COL_INV, PK_CRT, PK_CARRY, PK_LIN, PK_SCHOOL, PK_COUNT };
 

@@ -164,6 +164,16 @@ double ffg_last_decimal_ms(void);
    between calls (the next conversion recomputes them). */
 void ffg_decimal_cache_clear(void);
 
+/* Fingerprint of a number for checks on results too large to download or to
+   recompute (the format of the reference's tests/memrun.c:19-27): out[0] its
+   bit length, out[1] its low 64 bits, out[2 + k] its residue modulo
+   ffg_fp_primes[k] (18446744073709551557, 18446744073709551533,
+   9223372036854775783, 4611686018427387847).  Computed on the device; x a
+   device pointer (_device) or a host pointer (_host, copied in). */
+#define FFG_FP_PRIMES 4
+int ffg_fingerprint_device(const uint64_t *x, size_t n, uint64_t out[2 + FFG_FP_PRIMES]);
+int ffg_fingerprint_host(const uint64_t *x, size_t n, uint64_t out[2 + FFG_FP_PRIMES]);
+
 /* Words of the in-launch carry-settle ticket pool that are not zero (0 when
    the GPU is idle; a diagnostic). */
 int64_t ffg_tickets_in_use(void);

@@ -15,6 +15,8 @@ Sources (all produced here, none written by hand):
 * Decimal digits of F(10^6), F(10^7) and F(10^8) (sha256 and digit count)
   from the reference's big_to_string, each checked against Python's str().
   `--decimal-only` rewrites just that file.
+* `--add N` adds F(N)'s fingerprint (reference result, checked the same way)
+  to fingerprints.json: F(10^10) was added so (6.1 GB of host memory).
 """
 import hashlib
 import json
@@ -62,20 +64,26 @@ def binet_bits(n):
 
 
 def fingerprint_limbs(d):
-    x = 0
-    bits = 0
-    n = len(d)
-    while n > 1 and int(d[n - 1]) == 0:
-        n -= 1
-    top = int(d[n - 1])
-    bits = 64 * (n - 1) + top.bit_length()
-    out = [bits, int(d[0])]
-    for p in P4:
-        m = 0
-        for k in range(n - 1, -1, -1):
-            m = ((m << 64) | int(d[k])) % p
-        out.append(m)
-    return out
+    import numpy as np
+    x = int.from_bytes(np.ascontiguousarray(d, dtype=np.uint64).tobytes(), "little")
+    return [x.bit_length(), x & (2**64 - 1)] + [x % p for p in P4]
+
+
+def add_fingerprint(n):
+    """One more fingerprint (the reference's result, checked as in main)
+    merged into fingerprints.json."""
+    path = os.path.join(HERE, "fingerprints.json")
+    with open(path) as f:
+        gold = json.load(f)
+    d = Reference().fibonacci(n)
+    mine = fingerprint_limbs(d)
+    del d
+    indep = [binet_bits(n), fib_mod(n, 2**64)] + [fib_mod(n, p) for p in P4]
+    assert mine == indep, (n, mine, indep)
+    gold["fingerprints"][str(n)] = [str(v) for v in mine]
+    with open(path, "w") as f:
+        json.dump(gold, f, indent=1)
+    print("fingerprint", n, "ok", flush=True)
 
 
 def decimal_golden(ref):
@@ -95,6 +103,9 @@ def main():
     build(with_reference=True)
     if "--decimal-only" in sys.argv:
         decimal_golden(Reference())
+        return
+    if "--add" in sys.argv:
+        add_fingerprint(int(sys.argv[sys.argv.index("--add") + 1]))
         return
     from fibonacci import fibonacci  # the reference's Python oracle (fibonacci.py)
     ref = Reference()

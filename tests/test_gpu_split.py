@@ -72,3 +72,14 @@ def test_f1e9_split_cap23(ff, capped):
     x = limbs_to_int(ff.fibonacci(10**9))
     fp = [x.bit_length(), x & (2**64 - 1)] + [x % int(p) for p in gold["primes"]]
     assert [str(v) for v in fp] == gold["fingerprints"]["1000000000"]
+
+
+def test_f1e10(ff):
+    """F(10^10) (6.9 * 10^9 bits): the split at pieces of 2^25 past 32-bit
+    bit positions, against the reference-generated fingerprint; the 868 MB
+    result is fingerprinted on the device (its kernel is checked against
+    Python integers in test_gpu_fingerprint.py)."""
+    with open(os.path.join(GOLD, "fingerprints.json")) as f:
+        gold = json.load(f)
+    r = ff.fibonacci(10**10)
+    assert ff.fingerprint(r) == [int(v) for v in gold["fingerprints"]["10000000000"]]
