@@ -422,9 +422,11 @@ static void gpu_geometry(ffg_plan *pl) {
         pl->row_lg = t.c;
         return;
     }
+    // rows of 2^c and columns of at least 4: the split's pieces reach down to
+    // L = 16 when the transform cap is small (src/mul_split.c:160-161)
     int c = (int)pl->lg - 7;
     c = c < 8 ? 8 : (c > 13 ? 13 : c);
-    if (c > (int)pl->lg) c = (int)pl->lg;
+    if (c > (int)pl->lg - 2) c = (int)pl->lg - 2;
     pl->kernel = 1;
     pl->row_lg = (uint32_t)c;
 }

@@ -267,8 +267,18 @@ cudaError_t launch_conv_small(const Primes3 &P3, const ConvJobs &jobs, uint32_t 
     return cudaGetLastError();
 }
 
+// Geometry the four-step kernels support: lines of at least 2 words (a
+// stride-1 step has at least radix 2), rows of at least 4 words and column
+// tiles of 4..64 words within a row (16-byte row loads), tiles that fit
+// shared memory.
+static bool four_step_ok(const FourStep &G) {
+    return G.c >= 2 && G.c <= (uint32_t)FFG_LINE_LG && G.rn >= 1 && G.wc >= 4 && G.wc <= 64 &&
+           G.wc == (1u << G.wc_lg) && G.wc <= (1u << G.c) && (size_t)G.col_stride * G.wc * 4 <= 200 * 1024;
+}
+
 cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t njobs,
                              cudaStream_t st, double limb_bytes) {
+    if (!four_step_ok(G)) return cudaErrorInvalidValue;
     size_t sm_col = (size_t)G.col_stride * G.wc * sizeof(uint32_t);
     size_t sm_row = (size_t)line_stride(1u << G.c) * (G.square ? 1 : 2) * sizeof(uint32_t);
     cudaError_t e = smem_optin();
@@ -294,6 +304,7 @@ cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs 
 
 // The split multiply's passes, each over a list of jobs sharing geometry G.
 static cudaError_t cfg_four_step(const FourStep &G, size_t *sm_col, size_t *sm_row) {
+    if (!four_step_ok(G)) return cudaErrorInvalidValue;
     *sm_col = (size_t)G.col_stride * G.wc * sizeof(uint32_t);
     *sm_row = (size_t)line_stride(1u << G.c) * (G.square ? 1 : 2) * sizeof(uint32_t);
     return smem_optin();

@@ -83,3 +83,18 @@ def test_f1e10(ff):
         gold = json.load(f)
     r = ff.fibonacci(10**10)
     assert ff.fingerprint(r) == [int(v) for v in gold["fingerprints"]["10000000000"]]
+
+
+@pytest.mark.parametrize("lg", [4, 5, 6, 7, 8, 9])
+def test_split_tiny_pieces(ff, oracle, capped, lg):
+    """Transform caps of 2^4..2^9 (NTT_MAX_LG builds that low) split into
+    pieces as short as 16 coefficients: rows of 4 words, columns of 4."""
+    capped(lg)
+    rng = random.Random(100 + lg)
+    splits = 0
+    for na, nb in ((40, 40), (100, 37), (300, 300)):
+        x, y = rng.getrandbits(64 * na), rng.getrandbits(64 * nb)
+        splits += ff.plan(64 * na, 64 * nb)["split"]
+        assert limbs_to_int(ff.big_mul_ntt(int_to_limbs(x), int_to_limbs(y))) == x * y, (lg, na, nb)
+        assert limbs_to_int(ff.big_mul_ntt(int_to_limbs(x))) == x * x, (lg, na)
+    assert splits >= 1
