@@ -19,6 +19,8 @@
 // launch (the reference's step_proc / last_proc, src/fib.c:37-62, 123-143);
 // negative terms in two's complement (-s = ~s + 1 mod 2^(64 len)), so every
 // column sum is non-negative and the same ripple settle applies.
+#include <cstdlib>
+
 #include "ffg_internal.h"
 #include "ffg_ripple.cuh"
 
@@ -62,6 +64,35 @@ __global__ void __launch_bounds__(CRT_THREADS) k_crt_batch(GarnerConst K, const 
     crt_block(K, J, blockIdx.x);
 }
 
+// Garner's recombination of one coefficient's residues: X < p1 p2 p3 < 2^93.
+FFG_DEV_INLINE u128 garner(const GarnerConst &K, uint32_t r1, uint32_t r2, uint32_t r3) {
+    const uint32_t p1 = K.p[0], p2 = K.p[1], p3 = K.p[2];
+    const uint32_t x1m2 = min(r1, r1 - p2);
+    const uint32_t x2 = shoup(r2 - x1m2 + p2, K.i12, K.i12s, p2);
+    const uint32_t x1m3 = min(r1, r1 - p3);
+    const uint32_t t3 = shoup(r3 - x1m3 + p3, K.i13, K.i13s, p3);
+    const uint32_t x2m3 = min(x2, x2 - p3);
+    const uint32_t x3 = shoup(t3 - x2m3 + p3, K.i23, K.i23s, p3);
+    return (u128)((uint64_t)x2 * p1 + r1) + (u128)x3 * K.p12;
+}
+
+// Column sum lo + 2^64 hi of limb j (relative to the CTA's first limb) over
+// the values Z_i 2^(i b) (i relative to the CTA's first coefficient, stored
+// from -halo), every Z_i below 2^(top + 1).
+FFG_DEV_INLINE void column_sum(const uint64_t *Zlo, const uint32_t *Zhi, int32_t j, uint32_t b, int32_t halo,
+                               int32_t top, uint64_t &s_lo, uint32_t &s_hi) {
+    const int64_t ilo = floor_div(64 * (int64_t)j - top + b - 1, b), ihi = floor_div(64 * (int64_t)j + 63, b);
+    s_lo = 0;
+    s_hi = 0;
+    for (int64_t i = ilo < -halo ? -halo : ilo; i <= ihi; i++) {
+        const u128 X = ((u128)Zhi[i + halo] << 64) | Zlo[i + halo];
+        const int64_t sft = i * (int64_t)b - 64 * (int64_t)j;
+        const uint64_t part = sft >= 0 ? (uint64_t)(X << sft) : (uint64_t)(X >> (-sft));
+        s_lo += part;
+        s_hi += s_lo < part;
+    }
+}
+
 FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t cta) {
     extern __shared__ __align__(16) unsigned char sm[];
     uint64_t *Xlo = (uint64_t *)sm;                              // CRT_COEF + halo
@@ -74,7 +105,6 @@ FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t ct
     const uint32_t b = J.width, NL = CRT_NL_PER_W * b;
     const int32_t halo = (int32_t)(((156 + b - 1) / b + 1 + 3) & ~3u);
     const int64_t ibase = (int64_t)cta * CRT_COEF;
-    const uint32_t p1 = K.p[0], p2 = K.p[1], p3 = K.p[2];
 
     // residues in 16-byte vectors of 4 coefficients, every load of the thread
     // issued before any arithmetic (ibase - halo and the strides are multiples
@@ -102,17 +132,7 @@ FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t ct
 #pragma unroll
         for (int e = 0; e < 4; e++) {
             const int64_t gi = gi0 + e;
-            u128 X = 0;
-            if (gi >= 0 && (uint64_t)gi < J.conv) {
-                const uint32_t r1 = r1s[e], r2 = r2s[e], r3 = r3s[e];
-                const uint32_t x1m2 = min(r1, r1 - p2);
-                const uint32_t x2 = shoup(r2 - x1m2 + p2, K.i12, K.i12s, p2);
-                const uint32_t x1m3 = min(r1, r1 - p3);
-                const uint32_t t3 = shoup(r3 - x1m3 + p3, K.i13, K.i13s, p3);
-                const uint32_t x2m3 = min(x2, x2 - p3);
-                const uint32_t x3 = shoup(t3 - x2m3 + p3, K.i23, K.i23s, p3);
-                X = (u128)((uint64_t)x2 * p1 + r1) + (u128)x3 * K.p12;
-            }
+            const u128 X = gi >= 0 && (uint64_t)gi < J.conv ? garner(K, r1s[e], r2s[e], r3s[e]) : (u128)0;
             Xlo[4 * t4 + e] = (uint64_t)X;
             Xhi[4 * t4 + e] = (uint32_t)(X >> 64);
         }
@@ -123,16 +143,9 @@ FFG_DEV_INLINE void crt_block(const GarnerConst &K, const CrtJob &J, uint32_t ct
     const uint64_t j0 = (uint64_t)cta * NL;
     const bool neg_add = J.add < 0;
     for (int32_t j = (int32_t)threadIdx.x - 1; j < (int32_t)NL; j += blockDim.x) {
-        const int64_t ilo = floor_div(64 * (int64_t)j - 92 + b - 1, b), ihi = floor_div(64 * (int64_t)j + 63, b);
-        uint64_t s_lo = 0;
-        uint32_t s_hi = 0;
-        for (int64_t i = ilo < -halo ? -halo : ilo; i <= ihi; i++) {
-            const u128 X = ((u128)Xhi[i + halo] << 64) | Xlo[i + halo];
-            const int64_t s = i * (int64_t)b - 64 * (int64_t)j;
-            const uint64_t part = s >= 0 ? (uint64_t)(X << s) : (uint64_t)(X >> (-s));
-            s_lo += part;
-            s_hi += s_lo < part;
-        }
+        uint64_t s_lo;
+        uint32_t s_hi;
+        column_sum(Xlo, Xhi, j, b, halo, 92, s_lo, s_hi);
         // the constant: +add at limb 0, or 2^(64 nlimbs) + add when negative
         const int64_t jabs = (int64_t)j0 + j;
         if (J.add != 0 && jabs >= 0 && (uint64_t)jabs < J.nlimbs) {
@@ -214,6 +227,171 @@ cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_
     prof_begin(PK_CRT, st);
     k_crt_batch<<<dim3(max_ctas, count), CRT_THREADS, crt_smem(), st>>>(garner_const(), d_jobs);
     prof_end(PK_CRT, st, bytes);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------ CRT + linear pass
+//
+// k_crt_lin: the CRT of a doubling step's two squarings and the step's
+// linear pass in one launch.  With X1_i, X2_i the coefficients of s1 and s2,
+// output k is sum_i (alpha_k X1_i + beta_k X2_i) 2^(i b) + gamma_k.  beta_k
+// may be negative; every coefficient gets the bias B = K (2^b - 1), K =
+// 2^(94 - b), so that Z_i = alpha_k X1_i + beta_k X2_i + B >= 0 (|beta_k| X2_i
+// <= 2 p1 p2 p3 < 2^94 - K) and Z_i < 4 2^93 + 2^94 < 2^96.  Over the N
+// coefficients the CTAs cover, sum_i B 2^(i b) = K 2^(N b) - K: adding the
+// constant gamma_k + K leaves the output plus K 2^(N b), a multiple of
+// 2^(64 len) that falls off the top (N b >= 64 len).  A CTA recombines both
+// squarings' residues of its coefficients and writes one output (short
+// products: twice the CTAs, gridDim.y = 2) or both in turn (long products,
+// where recombining twice costs more than it hides).  The rest is crt_block
+// with values of up to 96 bits, and the CTA that finishes last settles both
+// outputs' carries.
+
+// Z_k of one coefficient gi from its residues in both squarings.
+FFG_DEV_INLINE u128 crt_lin_z(const GarnerConst &K, const CrtLinJob &J, uint32_t k, int64_t gi, u128 X1, u128 X2,
+                              u128 bias) {
+    if (gi < 0) return 0;
+    const uint64_t alpha = (uint64_t)(k ? J.alpha[1] : J.alpha[0]);
+    const int64_t beta = k ? J.beta[1] : J.beta[0];
+    // alpha > 0; beta of either sign, the sum taken mod 2^128 (exact: 0 <= Z < 2^96)
+    const u128 Z = X1 * alpha + bias;
+    return beta >= 0 ? Z + X2 * (uint64_t)beta : Z - X2 * (uint64_t)(-beta);
+}
+
+// kSplit: output blockIdx.y only, every load of the thread issued first
+// (short products: twice the CTAs); else both outputs from one
+// recombination, loads vector by vector (fewer registers, more CTAs per SM).
+template <bool kSplit>
+__global__ void __launch_bounds__(CRT_THREADS) k_crt_lin(GarnerConst K, CrtLinJob J) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    constexpr uint32_t ZN = CRT_COEF + CRT_HALO_MAX, NZ = kSplit ? 1 : 2;
+    uint64_t *Zlo0 = (uint64_t *)sm;                  // NZ x ZN
+    uint64_t *lo = Zlo0 + NZ * ZN;                    // NL limbs
+    uint32_t *Zhi0 = (uint32_t *)(lo + CRT_NL_MAX);   // NZ x ZN
+    uint32_t *hi = Zhi0 + NZ * ZN;                    // NL
+    uint32_t *gG = hi + CRT_NL_MAX, *gP = gG + CRT_NL_MAX / 32, *gin = gP + CRT_NL_MAX / 32;
+    __shared__ uint32_t hiprev_s;
+
+    const uint32_t kb = kSplit ? blockIdx.y : 0, ke = kSplit ? blockIdx.y + 1 : 2;
+    const uint32_t b = J.width, NL = CRT_NL_PER_W * b, cta = blockIdx.x;
+    const int32_t halo = (int32_t)(((159 + b - 1) / b + 1 + 3) & ~3u);
+    const int64_t ibase = (int64_t)cta * CRT_COEF;
+    const u128 bias = ((u128)1 << (94 - b)) * (((u128)1 << b) - 1);
+
+    constexpr int VPT = (CRT_COEF + CRT_HALO_MAX) / 4 / CRT_THREADS + 1;
+    constexpr int VPF = kSplit ? VPT : 1; // vectors whose loads are in flight together
+    const int32_t nvec = ((int32_t)CRT_COEF + halo) / 4;
+#pragma unroll
+    for (int v0 = 0; v0 < VPT; v0 += VPF) {
+        uint4 rv[VPF][2][3];
+#pragma unroll
+        for (int v = 0; v < VPF; v++) {
+            const int32_t t4 = (int32_t)threadIdx.x + (v0 + v) * (int32_t)blockDim.x;
+            const int64_t gi = ibase - halo + 4 * (int64_t)t4;
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const bool in = t4 < nvec && gi >= 0 && (uint64_t)gi < J.conv[q];
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    rv[v][q][c] = in ? __ldg((const uint4 *)(J.y[q] + c * J.y_stride + gi)) : make_uint4(0, 0, 0, 0);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < VPF; v++) {
+            const int32_t t4 = (int32_t)threadIdx.x + (v0 + v) * (int32_t)blockDim.x;
+            if (t4 >= nvec) break;
+            const int64_t gi0 = ibase - halo + 4 * (int64_t)t4;
+            const uint32_t r[2][3][4] = {{{rv[v][0][0].x, rv[v][0][0].y, rv[v][0][0].z, rv[v][0][0].w},
+                                          {rv[v][0][1].x, rv[v][0][1].y, rv[v][0][1].z, rv[v][0][1].w},
+                                          {rv[v][0][2].x, rv[v][0][2].y, rv[v][0][2].z, rv[v][0][2].w}},
+                                         {{rv[v][1][0].x, rv[v][1][0].y, rv[v][1][0].z, rv[v][1][0].w},
+                                          {rv[v][1][1].x, rv[v][1][1].y, rv[v][1][1].z, rv[v][1][1].w},
+                                          {rv[v][1][2].x, rv[v][1][2].y, rv[v][1][2].z, rv[v][1][2].w}}};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int64_t gi = gi0 + e;
+                u128 X1 = 0, X2 = 0;
+                if (gi >= 0) {
+                    X1 = (uint64_t)gi < J.conv[0] ? garner(K, r[0][0][e], r[0][1][e], r[0][2][e]) : (u128)0;
+                    X2 = (uint64_t)gi < J.conv[1] ? garner(K, r[1][0][e], r[1][1][e], r[1][2][e]) : (u128)0;
+                }
+#pragma unroll
+                for (uint32_t z = 0; z < NZ; z++) {
+                    const u128 Z = crt_lin_z(K, J, kb + z, gi, X1, X2, bias);
+                    Zlo0[z * ZN + 4 * t4 + e] = (uint64_t)Z;
+                    Zhi0[z * ZN + 4 * t4 + e] = (uint32_t)(Z >> 64);
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    const uint64_t j0 = (uint64_t)cta * NL;
+    const uint32_t ncta = gridDim.x;
+    for (uint32_t k = kb; k < ke; k++) {
+        const uint32_t z = k - kb;
+        const uint64_t add = (uint64_t)(k ? J.gamma[1] : J.gamma[0]) + ((uint64_t)1 << (94 - b)); // gamma + K > 0
+        for (int32_t j = (int32_t)threadIdx.x - 1; j < (int32_t)NL; j += blockDim.x) {
+            uint64_t s_lo;
+            uint32_t s_hi;
+            column_sum(Zlo0 + z * ZN, Zhi0 + z * ZN, j, b, halo, 95, s_lo, s_hi);
+            if (cta == 0 && j == 0) {
+                s_lo += add;
+                s_hi += s_lo < add;
+            }
+            if (j < 0) hiprev_s = s_hi;
+            else {
+                lo[j] = s_lo;
+                hi[j] = s_hi;
+            }
+        }
+        __syncthreads();
+        const uint32_t map = cta_resolve(lo, hi, cta ? hiprev_s : 0, NL, gG, gP, gin);
+        uint64_t *out = k ? J.out[1] : J.out[0];
+        for (uint32_t j = threadIdx.x; j < NL && j0 + j < J.len; j += blockDim.x) out[j0 + j] = lo[j];
+        if (threadIdx.x == 0) J.maps[(size_t)k * ncta + cta] = map;
+        __syncthreads();
+    }
+    if (ncta > 1 && last_cta(J.ticket, ncta * gridDim.y)) {
+        for (int q = 0; q < 2; q++) settle_cta(q ? J.out[1] : J.out[0], J.len, NL, J.maps + (size_t)q * ncta, ncta);
+        if (threadIdx.x == 0) *J.ticket = 0;
+    }
+}
+
+static size_t crt_lin_smem(bool split) {
+    return (split ? 1 : 2) * (CRT_COEF + CRT_HALO_MAX) * (8 + 4) + CRT_NL_MAX * (8 + 4) + 3 * (CRT_NL_MAX / 32) * 4;
+}
+
+// Products of up to this many CTAs per output run one output per CTA
+// (measured on the F(10^8) and F(10^9) chains).
+static uint32_t crt_lin_split_max() {
+    static long v = -1;
+    if (v < 0) {
+        const char *e = getenv("FFG_CRT_LIN_SPLIT");
+        v = e && *e ? strtol(e, nullptr, 10) : 128;
+        if (v < 0) v = 0;
+    }
+    return (uint32_t)v;
+}
+
+cudaError_t launch_crt_lin(const CrtLinJob &J, cudaStream_t st) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_crt_lin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)crt_lin_smem(true));
+        if (!e)
+            e = cudaFuncSetAttribute(k_crt_lin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)crt_lin_smem(false));
+        if (e) return e;
+        configured = true;
+    }
+    if (J.width < 32 || J.width > 35 || J.alpha[0] <= 0 || J.alpha[1] <= 0) return cudaErrorInvalidValue;
+    const uint32_t ncta = crt_ctas(J.len, J.width);
+    const bool split = ncta <= crt_lin_split_max();
+    prof_begin(PK_CRT, st);
+    if (split) k_crt_lin<true><<<dim3(ncta, 2), CRT_THREADS, crt_lin_smem(true), st>>>(garner_const(), J);
+    else k_crt_lin<false><<<dim3(ncta, 1), CRT_THREADS, crt_lin_smem(false), st>>>(garner_const(), J);
+    prof_end(PK_CRT, st, 12.0 * (double)(J.conv[0] + J.conv[1]) + 16.0 * (double)J.len);
     return cudaGetLastError();
 }
 

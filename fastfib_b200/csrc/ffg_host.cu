@@ -526,7 +526,17 @@ static FourStep four_step_geometry(const ffg_plan &pl, bool square) {
 
 // Products that share one plan (same width, length, squareness), run as one
 // batch of transforms, then one CRT each.
-static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool square, cudaStream_t st) {
+// A doubling step's linear pass fused into the CRT of its two squarings
+// (k_crt_lin): out_k = alpha_k s1 + beta_k s2 + gamma_k over len limbs.
+struct LinFuse {
+    uint64_t *out[2];
+    uint64_t len;
+    int32_t alpha[2], beta[2];
+    int64_t gamma[2];
+};
+
+static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool square, cudaStream_t st,
+                        const LinFuse *fuse = nullptr) {
     const uint64_t L = pl.L;
     uint32_t scl[3], scls[3];
     scale_consts(L, scl, scls);
@@ -592,6 +602,26 @@ static int run_products(const Prod *pr, int count, const ffg_plan &pl, bool squa
         C.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(C.nlimbs, w) * sizeof(uint32_t));
         if (!C.maps) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
         C.ticket = ticket_get();
+    }
+    if (fuse && count == 2) {
+        CrtLinJob F{};
+        for (int q = 0; q < 2; q++) {
+            F.y[q] = crt[q].y;
+            F.conv[q] = crt[q].conv;
+            F.out[q] = fuse->out[q];
+            F.alpha[q] = fuse->alpha[q];
+            F.beta[q] = fuse->beta[q];
+            F.gamma[q] = fuse->gamma[q];
+        }
+        F.y_stride = L;
+        F.len = fuse->len;
+        F.width = w;
+        F.maps = (uint32_t *)arena_alloc(2 * (size_t)crt_ctas(F.len, w) * sizeof(uint32_t));
+        if (!F.maps) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
+        F.ticket = ticket_get();
+        e = launch_crt_lin(F, st);
+        if (e) return fail(FFG_E_CUDA, "crt + linear pass: %s", cudaGetErrorString(e));
+        return FFG_OK;
     }
     for (int i = 0; i < count; i += 2) { // the step's pair in one launch
         e = launch_crt_pair(crt + i, count - i >= 2 ? 2 : 1, st);
@@ -731,6 +761,17 @@ static int lin(const uint64_t *s1, uint64_t n1, const uint64_t *s2, uint64_t n2,
     return FFG_OK;
 }
 
+// FFG_NO_CRT_LIN=1: the step's CRT pair and linear pass as two launches
+// (the same results; for comparing the two).
+static bool crt_lin_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("FFG_NO_CRT_LIN");
+        on = !(e && *e && *e != '0');
+    }
+    return on != 0;
+}
+
 // The device part of the chain, from the pair (F(k-1), F(k)) in fkm1 / fk
 // (bit lengths bkm1 / bk) to F(n) in *res (*nres limbs, leading zeros
 // allowed): kernel launches and arena allocations only, in the same order on
@@ -772,6 +813,33 @@ static int chain_body(uint64_t n, int i0, uint64_t *fk, uint64_t *fkm1, uint64_t
         } else if (pl1.split || pl2.split) {
             rc = mul_one(p1, true, st);
             if (!rc) rc = mul_one(p2, true, st);
+        } else if (pl1.width == pl2.width && pl1.L == pl2.L && pl1.kernel == pl2.kernel &&
+                   pl1.row_lg == pl2.row_lg && crt_lin_enabled()) {
+            // both squarings in one launch set; the CRT writes the step's
+            // two results directly (k_crt_lin)
+            Prod pp[2] = {p1, p2};
+            const uint64_t len = n1 + 1;
+            const int64_t pm2 = kodd ? -2 : 2;
+            ALLOC(lo, uint64_t, len);
+            ALLOC(hi, uint64_t, len);
+            LinFuse fz{};
+            fz.out[0] = lo, fz.out[1] = hi, fz.len = len;
+            if (bit) {
+                fz.alpha[0] = 3, fz.beta[0] = -2, fz.gamma[0] = pm2;
+                fz.alpha[1] = 4, fz.beta[1] = -1, fz.gamma[1] = pm2;
+            } else {
+                fz.alpha[0] = 1, fz.beta[0] = 1, fz.gamma[0] = 0;
+                fz.alpha[1] = 3, fz.beta[1] = -2, fz.gamma[1] = pm2;
+            }
+            rc = run_products(pp, 2, pl1, true, st, &fz);
+            if (rc) return rc;
+            k = 2 * k + (uint64_t)bit;
+            kodd = bit;
+            fkm1 = lo;
+            fk = hi;
+            bk = fib_bits(k);
+            bkm1 = fib_bits(k - 1);
+            continue;
         } else if (pl1.width == pl2.width && pl1.L == pl2.L && pl1.kernel == pl2.kernel &&
                    pl1.row_lg == pl2.row_lg) {
             Prod pp[2] = {p1, p2};

@@ -98,6 +98,24 @@ struct LinJob {
     uint32_t *ticket;        // a zero word of the ticket pool (ticket_get)
 };
 
+// The CRT of a fast-doubling step's two squarings fused with its linear
+// pass: out_k = alpha_k s1 + beta_k s2 + gamma_k (k = 0, 1, len limbs each)
+// straight from the residues of s1 = y[0] and s2 = y[1] (same width and
+// length), without writing s1 and s2.
+struct CrtLinJob {
+    const uint32_t *y[2];
+    uint64_t y_stride;
+    uint64_t conv[2];
+    uint64_t *out[2];
+    uint64_t len;
+    uint32_t width;
+    uint32_t pad;
+    int32_t alpha[2], beta[2];
+    int64_t gamma[2];
+    uint32_t *maps;          // 2 * crt_ctas(len, width) words
+    uint32_t *ticket;        // a zero word of the ticket pool (ticket_get)
+};
+
 // Jobs travel to the kernels by value, as kernel parameters: nothing is
 // copied to the device per launch, so launches queue up without waiting and
 // a whole chain can be captured into a CUDA graph.
@@ -211,6 +229,7 @@ cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob &job, 
 cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st);
 cudaError_t launch_crt_pair(const CrtJob *jobs, uint32_t count, cudaStream_t st); // count 1 or 2, by value
 cudaError_t launch_lin(const LinJob &J, cudaStream_t st);
+cudaError_t launch_crt_lin(const CrtLinJob &J, cudaStream_t st);
 
 // The cost model's kernels (ffg_mlp.cu); parameters, rows and outputs on the device.
 cudaError_t launch_mlp_train(float *d_params, const float *d_X, const int32_t *d_M, const float *d_Y, uint32_t n,
