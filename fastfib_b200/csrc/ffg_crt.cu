@@ -498,6 +498,121 @@ cudaError_t launch_school_pair(const SchoolJob *jobs, uint32_t count, cudaStream
     return cudaGetLastError();
 }
 
+// k_school_sq_pair: the doubling step's two short squarings (operands of up
+// to a few hundred limbs) spread over more CTAs than k_school_pair gives
+// them: SQ_NL = 64 output limbs per CTA, 4 threads per column, and the
+// symmetry of a square: column j = 2 sum_{i < j - i} a_i a_(j-i) + a_(j/2)^2
+// (j even).  The same 192-bit column sums, ripple settle and last-CTA carry
+// settle as k_school.
+constexpr uint32_t SQ_NL = 64;
+constexpr uint32_t SQ_TPC = 4; // threads per column
+
+__host__ __device__ uint32_t school_sq_ctas(uint64_t nlimbs) { return (uint32_t)((nlimbs + SQ_NL - 1) / SQ_NL); }
+
+__global__ void __launch_bounds__(SCHOOL_THREADS) k_school_sq_pair(SchoolPair Pr) {
+    const SchoolJob &J = blockIdx.y ? Pr.j[1] : Pr.j[0];
+    const uint32_t ncta = school_sq_ctas(J.nlimbs);
+    if (blockIdx.x >= ncta) return;
+    constexpr uint32_t NC = SQ_NL + 3; // columns j0 - 3 .. j0 + SQ_NL - 1
+    __shared__ uint64_t p0[NC][SQ_TPC], p1[NC][SQ_TPC];
+    __shared__ uint32_t p2[NC][SQ_TPC];
+    __shared__ uint64_t t0s[NC], t1s[NC];
+    __shared__ uint32_t t2s[NC];
+    __shared__ uint64_t lo[SQ_NL];
+    __shared__ uint32_t hi[SQ_NL];
+    __shared__ uint32_t gG[SQ_NL / 32], gP[SQ_NL / 32], gin[SQ_NL / 32];
+    __shared__ uint32_t hiprev_s;
+    const int64_t j0 = (int64_t)blockIdx.x * SQ_NL, n = (int64_t)J.na;
+    const uint64_t *a = J.a;
+    // partial sums of a_i a_(j-i) over i < j - i, i = part (mod SQ_TPC)
+    for (uint32_t slot = threadIdx.x; slot < NC * SQ_TPC; slot += blockDim.x) {
+        const uint32_t c = slot / SQ_TPC, part = slot % SQ_TPC;
+        const int64_t j = j0 - 3 + (int64_t)c;
+        uint64_t t0 = 0, t1 = 0, t2 = 0;
+        if (j >= 1 && j <= 2 * n - 3) {
+            const int64_t ilo = j - n + 1 > 0 ? j - n + 1 : 0, ihi = (j - 1) / 2; // i < j - i
+            for (int64_t i = ilo + part; i <= ihi; i += SQ_TPC) {
+                const u128 pr = (u128)__ldg(&a[i]) * __ldg(&a[j - i]);
+                const uint64_t l = (uint64_t)pr, h = (uint64_t)(pr >> 64);
+                t0 += l;
+                const uint64_t hh = h + (t0 < l);
+                t1 += hh;
+                t2 += t1 < hh;
+            }
+        }
+        p0[c][part] = t0;
+        p1[c][part] = t1;
+        p2[c][part] = (uint32_t)t2;
+    }
+    __syncthreads();
+    // column j: 2 S_j + a_(j/2)^2, in 192 bits
+    for (uint32_t c = threadIdx.x; c < NC; c += blockDim.x) {
+        const int64_t j = j0 - 3 + (int64_t)c;
+        uint64_t t0 = 0, t1 = 0, t2 = 0;
+        for (uint32_t q = 0; q < SQ_TPC; q++) {
+            t0 += p0[c][q];
+            const uint64_t c0 = t0 < p0[c][q];
+            const uint64_t x1 = p1[c][q] + c0; // p1 < 2^64 - 1 is not assured: carry both ways
+            const uint64_t c1 = x1 < c0;
+            t1 += x1;
+            t2 += p2[c][q] + c1 + (t1 < x1);
+        }
+        // doubled
+        t2 = (t2 << 1) | (t1 >> 63);
+        t1 = (t1 << 1) | (t0 >> 63);
+        t0 <<= 1;
+        if (j >= 0 && j <= 2 * n - 2 && (j & 1) == 0) {
+            const uint64_t x = __ldg(&a[j / 2]);
+            const u128 sq = (u128)x * x;
+            const uint64_t l = (uint64_t)sq, h = (uint64_t)(sq >> 64);
+            t0 += l;
+            const uint64_t c0 = t0 < l;
+            const uint64_t x1 = h + c0;
+            const uint64_t c1 = x1 < c0;
+            t1 += x1;
+            t2 += c1 + (t1 < x1);
+        }
+        t0s[c] = t0;
+        t1s[c] = t1;
+        t2s[c] = (uint32_t)t2;
+    }
+    __syncthreads();
+    // v_j = t0_j + t1_(j-1) + t2_(j-2), for j = j0 - 1 .. j0 + SQ_NL - 1
+    for (int32_t jl = (int32_t)threadIdx.x - 1; jl < (int32_t)SQ_NL; jl += blockDim.x) {
+        const uint32_t c = (uint32_t)(jl + 3);
+        const u128 v = (u128)t0s[c] + t1s[c - 1] + t2s[c - 2];
+        if (jl < 0) hiprev_s = (uint32_t)(v >> 64);
+        else {
+            lo[jl] = (uint64_t)v;
+            hi[jl] = (uint32_t)(v >> 64);
+        }
+    }
+    __syncthreads();
+    const uint32_t map = cta_resolve(lo, hi, blockIdx.x ? hiprev_s : 0, SQ_NL, gG, gP, gin);
+    for (uint32_t j = threadIdx.x; j < SQ_NL && (uint64_t)j0 + j < J.nlimbs; j += blockDim.x) J.out[j0 + j] = lo[j];
+    if (threadIdx.x == 0) J.maps[blockIdx.x] = map;
+    if (ncta > 1 && last_cta(J.ticket, ncta)) {
+        settle_cta(J.out, J.nlimbs, SQ_NL, J.maps, ncta);
+        if (threadIdx.x == 0) *J.ticket = 0;
+    }
+}
+
+cudaError_t launch_school_sq_pair(const SchoolJob *jobs, uint32_t count, cudaStream_t st) {
+    SchoolPair P{};
+    uint32_t mx = 0;
+    double bytes = 0;
+    for (uint32_t i = 0; i < count && i < 2; i++) {
+        if (jobs[i].a != jobs[i].b || jobs[i].na != jobs[i].nb) return cudaErrorInvalidValue;
+        P.j[i] = jobs[i];
+        mx = max(mx, school_sq_ctas(jobs[i].nlimbs));
+        bytes += 8.0 * (double)(jobs[i].na + jobs[i].nlimbs);
+    }
+    prof_begin(PK_SCHOOL, st);
+    k_school_sq_pair<<<dim3(mx, count), SCHOOL_THREADS, 0, st>>>(P);
+    prof_end(PK_SCHOOL, st, bytes);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
                                 double bytes) {
     if (!count) return cudaSuccess;

@@ -804,11 +804,11 @@ static int chain_body(uint64_t n, int i0, uint64_t *fk, uint64_t *fkm1, uint64_t
                 J.na = J.nb = (pp[q]->bits_a + 63) / 64;
                 J.out = pp[q]->out;
                 J.nlimbs = 2 * pp[q]->na + 1;
-                J.maps = (uint32_t *)arena_alloc((size_t)school_ctas(J.nlimbs) * 4);
+                J.maps = (uint32_t *)arena_alloc((size_t)school_sq_ctas(J.nlimbs) * 4);
                 if (!J.maps) return fail(FFG_E_NOMEM, "device arena: schoolbook maps");
                 J.ticket = ticket_get();
             }
-            cudaError_t e = launch_school_pair(sj, 2, st);
+            cudaError_t e = launch_school_sq_pair(sj, 2, st);
             if (e) return fail(FFG_E_CUDA, "schoolbook pair: %s", cudaGetErrorString(e));
         } else if (pl1.split || pl2.split) {
             rc = mul_one(p1, true, st);

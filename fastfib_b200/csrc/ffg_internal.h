@@ -213,7 +213,11 @@ __host__ __device__ uint32_t school_ctas(uint64_t nlimbs); // CTAs (and carry ma
 // Batches in device arrays: one launch (plus one settle) for all products.
 cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
                              double bytes);
-cudaError_t launch_school_pair(const SchoolJob *jobs, uint32_t count, cudaStream_t st); // 1 or 2, by value
+cudaError_t launch_school_pair(const SchoolJob *jobs, uint32_t count, cudaStream_t st);
+// The doubling step's two short squarings (a == b), SQ_NL output limbs per
+// CTA: school_sq_ctas(nlimbs) words of maps each.
+cudaError_t launch_school_sq_pair(const SchoolJob *jobs, uint32_t count, cudaStream_t st);
+__host__ __device__ uint32_t school_sq_ctas(uint64_t nlimbs); // 1 or 2, by value
 cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
                                 double bytes);
 uint32_t lin_ctas(uint64_t len);                    // CTAs of one linear pass
