@@ -32,6 +32,16 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC = os.path.join(ROOT, "profiles", "roofline_traffic.json")
 METRIC = "F(n) ms at n=1e8/1e9 on 1 B200, bit-exact; learned vs plain; NTT % HBM peak"
 PUBLISHED_F1E8_MS = 46.0  # the reference's README, F(10^8) on an i9-9900K
+FALLBACK_HBM_GBS = 6650.0  # an earlier copy-bandwidth measurement on B200
+
+
+def hbm_peak():
+    """(GB/s, source): the measured copy bandwidth from MEASURED_PEAKS.json
+    when it is present, else the earlier measurement."""
+    if os.path.exists(PEAKS):
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return FALLBACK_HBM_GBS, "fallback (6.65 TB/s; MEASURED_PEAKS.json absent)"
 
 
 def workload(n):
@@ -225,8 +235,7 @@ def ntt_microbench(limbs, square, steps, warmup):
     with open(GOLD_FP) as f:
         primes = [int(p) for p in json.load(f)["primes"]]
     ok = all(z % p == (x % p) * ((x if sq else y) % p) % p for p in primes) and z.bit_length() <= 128 * n
-    with open(PEAKS) as f:
-        peak = json.load(f)["hbm_gbs"]
+    peak, peak_src = hbm_peak()
     fam = {k: {"launches": v["launches"], "ms_per_launch": v["ms"] / max(1, v["launches"]),
                "gbs": v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else 0.0,
                "frac": (v["bytes"] / (v["ms"] * 1e-3) / 1e9 / peak) if v["ms"] else 0.0}
@@ -241,7 +250,7 @@ def ntt_microbench(limbs, square, steps, warmup):
             "bit_exact": ok, "families": fam, "peak_gbs": peak,
             "ntt_passes": {"gbs": pb / (pm * 1e-3) / 1e9 if pm else 0.0,
                            "frac": (pb / (pm * 1e-3) / 1e9 / peak) if pm else 0.0,
-                           "of": "measured (MEASURED_PEAKS.json hbm_gbs)"}}
+                           "of": peak_src}}
 
 
 def job_ms(totals, steps, world, device="cuda"):
@@ -416,10 +425,12 @@ def main():
         if world > 1:
             dist.barrier()
 
-    # warm-up: tables, arena, which kernel family dominates, then the chain's
-    # CUDA graph (captured on its second run with the timed profiling mask)
-    ff.profile(True)
+    # warm-up: tables, arena and every kernel loaded; then which kernel family
+    # dominates (a profiled run after the warm one), then the chain's CUDA
+    # graph (captured on its second run with the timed profiling mask)
     r = ff.fibonacci(args.n)
+    ff.profile(True)
+    ff.fibonacci(args.n)
     prof = ff.profile_read()
     dominant = max(prof, key=lambda k: prof[k]["ms"])
     ok = fingerprint_ok(args.n, r)
@@ -489,8 +500,7 @@ def main():
         extra["f1e10_split"] = big(10**10, device_fp=True)
 
     if rank == 0:
-        with open(PEAKS) as f:
-            peak = json.load(f)["hbm_gbs"]
+        peak, peak_src = hbm_peak()
         achieved = prof["bytes"] / (prof["ms"] * 1e-3) / 1e9 if prof["ms"] > 0 else 0.0
         traffic = None
         if os.path.exists(TRAFFIC):
@@ -503,7 +513,7 @@ def main():
             "data": "synthetic (F(n) needs no input data)", "config": workload(args.n),
             "bit_exact": ok,
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)",
+                         "frac": achieved / peak, "peak_source": peak_src,
                          "traffic": traffic, "launches": prof["launches"],
                          "algorithmic_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]),
                          "ms_per_launch": prof["ms"] / max(1, prof["launches"])},
