@@ -274,9 +274,20 @@ def to_decimal(a, device_ptr: int = 0, n: int = 0):
                                          ctypes.byref(done)))
     if not done.value:
         return None, False
-    s = ctypes.string_at(out.value, nout.value).decode()
+    s = _ascii_str(out.value, nout.value)
     ctypes.CDLL(None).free(out)
     return s, True
+
+
+_decode_ascii = ctypes.pythonapi.PyUnicode_DecodeASCII
+_decode_ascii.restype = ctypes.py_object
+_decode_ascii.argtypes = [ctypes.c_void_p, ctypes.c_ssize_t, ctypes.c_char_p]
+
+
+def _ascii_str(ptr: int, n: int) -> str:
+    """A Python str of the n ASCII bytes at ptr, decoded in one pass (no
+    intermediate bytes object)."""
+    return _decode_ascii(ptr, n, None)
 
 
 # ------------------------------------------------------------------ the GPU ABI

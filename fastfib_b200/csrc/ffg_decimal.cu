@@ -19,6 +19,8 @@
 //                   invariant integer, Moller and Granlund, IEEE Trans.
 //                   Computers 60(2), 2011, algorithm 4), one thread a piece
 //   k_bit_length  : the bit length of one number (the powers' sizes)
+#include <cstring>
+
 #include "ffg_internal.h"
 #include "ffg_ripple.cuh"
 
@@ -223,7 +225,7 @@ FFG_DEV_INLINE uint64_t div_2by1(uint64_t u1, uint64_t u0, uint64_t v, uint64_t 
     return q1;
 }
 
-__global__ void __launch_bounds__(128) k_leaf_digits(const LeafJob *__restrict__ jobs, uint32_t count, uint32_t chunks,
+__global__ void __launch_bounds__(32) k_leaf_digits(const LeafJob *__restrict__ jobs, uint32_t count, uint32_t chunks,
                                                       uint64_t v, char *out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
@@ -250,42 +252,59 @@ cudaError_t launch_leaf_digits(const LeafJob *d_jobs, uint32_t count, uint32_t c
                                cudaStream_t st) {
     if (!count) return cudaSuccess;
     prof_begin(PK_LIN, st);
-    k_leaf_digits<<<(count + 127) / 128, 128, 0, st>>>(d_jobs, count, chunks, v, d_out);
+    // one thread a leaf, one warp a CTA: the leaves' serial divisions spread
+    // over every SM instead of a quarter as many
+    k_leaf_digits<<<(count + 31) / 32, 32, 0, st>>>(d_jobs, count, chunks, v, d_out);
     prof_end(PK_LIN, st, (double)count * chunks * 19);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------- leading zeros
 
-__global__ void k_first_nonzero(const char *d, uint64_t n, unsigned long long *first) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        if (d[i] != '0') {
-            atomicMin(first, (unsigned long long)i);
-            return;
+// The first digit that is not '0': each thread scans 16-byte groups (grid
+// stride) and stops at its first find, the block keeps its minimum, and one
+// atomic per block publishes it.  d is 16-byte aligned.
+__global__ void __launch_bounds__(256) k_first_nonzero(const char *d, uint64_t n, unsigned long long *first) {
+    __shared__ unsigned long long best;
+    if (threadIdx.x == 0) best = ~0ull;
+    __syncthreads();
+    const uint64_t groups = (n + 15) / 16, stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += stride) {
+        const uint64_t i0 = 16 * g;
+        uint4 v;
+        if (i0 + 16 <= n) v = *(const uint4 *)(d + i0);
+        else {
+            unsigned char b[16];
+            for (int k = 0; k < 16; k++) b[k] = i0 + k < n ? (unsigned char)d[i0 + k] : (unsigned char)'0';
+            memcpy(&v, b, 16);
         }
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        int hit = -1;
+        for (int k = 0; k < 16 && hit < 0; k++)
+            if (((w[k >> 2] >> (8 * (k & 3))) & 0xffu) != (uint32_t)'0') hit = k;
+        if (hit >= 0) {
+            atomicMin(&best, (unsigned long long)(i0 + hit));
+            break;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && best != ~0ull) atomicMin(first, best);
 }
 
 cudaError_t launch_first_nonzero(const char *d, uint64_t n, unsigned long long *d_first, cudaStream_t st) {
-    uint64_t blocks = (n + 255) / 256;
-    k_first_nonzero<<<(uint32_t)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(d, n, d_first);
+    const uint64_t blocks = (n + 16 * 256 - 1) / (16 * 256);
+    k_first_nonzero<<<(uint32_t)(blocks < 592 ? (blocks ? blocks : 1) : 592), 256, 0, st>>>(d, n, d_first);
     return cudaGetLastError();
 }
 
 // ------------------------------------------------------------ bit length
 
-__global__ void k_bit_length(const uint64_t *x, uint64_t n, uint64_t *out) {
-    __shared__ unsigned long long best;
-    if (threadIdx.x == 0) best = 0;
-    __syncthreads();
-    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x)
-        if (x[i]) atomicMax(&best, (unsigned long long)(64 * i + 64 - __clzll(x[i])));
-    __syncthreads();
-    if (threadIdx.x == 0) *out = best;
-}
-
+// Bit length of x into *d_out: the multi-block scan of ffg_fingerprint.cu
+// (one atomic maximum per thread) on a zeroed word.
 cudaError_t launch_bit_length(const uint64_t *x, uint64_t n, uint64_t *d_out, cudaStream_t st) {
-    k_bit_length<<<1, 1024, 0, st>>>(x, n, d_out);
-    return cudaGetLastError();
+    cudaError_t e = cudaMemsetAsync(d_out, 0, 8, st);
+    if (e) return e;
+    return launch_bits_mb(x, n, (unsigned long long *)d_out, st);
 }
 
 } // namespace ffg

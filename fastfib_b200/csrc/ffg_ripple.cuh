@@ -97,12 +97,23 @@ FFG_DEV_INLINE uint32_t cta_resolve(uint64_t *lo, const uint32_t *hi, uint32_t h
 // threads): thread t composes the maps of its run of consecutive CTAs, a
 // block-wide scan of those composites gives the carry into every run (carry
 // 0 into the first CTA), and each thread walks its run again adding the
-// carry into the CTAs that receive one (a carry stops at the first limb that
-// does not wrap).  Maps and limbs written by other CTAs are read through L2.
+// carry into the CTAs that receive one: a carry stops at the first limb that
+// does not wrap, almost always the first.  A carry still running after
+// kSettleWalk limbs (a CTA whose limbs are mostly 2^64 - 1, which Barrett and
+// Newton combinations produce) is finished by the whole block afterwards,
+// 256 limbs at a time, so no thread walks thousands of dependent loads.
+// Maps and limbs written by other CTAs are read through L2.
+constexpr uint32_t kSettleWalk = 8;
+constexpr uint32_t kSettleLong = 64;
+
 FFG_DEV_INLINE void settle_cta(uint64_t *out, uint64_t nlimbs, uint32_t cta_limbs, const uint32_t *maps,
                                uint32_t ncta) {
     __shared__ uint32_t wpre[32];
+    __shared__ uint64_t long_j[kSettleLong], long_end[kSettleLong];
+    __shared__ uint32_t nlong;
+    __shared__ uint64_t first_s;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) nlong = 0;
     const uint32_t per = (ncta + blockDim.x - 1) / blockDim.x;
     const uint32_t q0 = min(ncta, threadIdx.x * per), q1 = min(ncta, q0 + per);
     uint32_t run = 2u; // identity: c -> c
@@ -123,13 +134,50 @@ FFG_DEV_INLINE void settle_cta(uint64_t *out, uint64_t nlimbs, uint32_t cta_limb
     for (uint32_t q = q0; q < q1; q++) {
         if (carry) {
             const uint64_t end = min(nlimbs, (uint64_t)(q + 1) * cta_limbs);
-            for (uint64_t j = (uint64_t)q * cta_limbs; j < end; j++) {
+            uint64_t j = (uint64_t)q * cta_limbs;
+            bool running = true;
+            for (uint32_t w = 0; w < kSettleWalk && j < end; w++, j++) {
                 const uint64_t v = __ldcg(&out[j]) + 1;
                 out[j] = v;
-                if (v != 0) break;
+                if (v != 0) {
+                    running = false;
+                    break;
+                }
+            }
+            if (running && j < end) {
+                const uint32_t slot = atomicAdd(&nlong, 1u);
+                if (slot < kSettleLong) {
+                    long_j[slot] = j;
+                    long_end[slot] = end;
+                } else { // list full: finish here
+                    for (; j < end; j++) {
+                        const uint64_t v = __ldcg(&out[j]) + 1;
+                        out[j] = v;
+                        if (v != 0) break;
+                    }
+                }
             }
         }
         carry = map_apply(__ldcg(&maps[q]), carry);
+    }
+    __syncthreads();
+    // the long carries, one at a time by the whole block: limbs before the
+    // first one that is not 2^64 - 1 become 0, that one gains 1
+    const uint32_t nl = min(nlong, kSettleLong);
+    for (uint32_t e = 0; e < nl; e++) {
+        const uint64_t end = long_end[e];
+        for (uint64_t base = long_j[e]; base < end; base += blockDim.x) {
+            if (threadIdx.x == 0) first_s = ~0ull;
+            __syncthreads();
+            const uint64_t j = base + threadIdx.x;
+            const uint64_t v = j < end ? __ldcg(&out[j]) : 0;
+            if (j < end && v != ~0ull) atomicMin((unsigned long long *)&first_s, (unsigned long long)j);
+            __syncthreads();
+            const uint64_t first = first_s;
+            if (j < end && j <= first) out[j] = j == first ? v + 1 : 0;
+            __syncthreads(); // first_s is reused
+            if (first != ~0ull) break;
+        }
     }
     __syncthreads();
 }

@@ -17,6 +17,13 @@ import subprocess
 
 import numpy as np
 
+_libc = ctypes.CDLL(None)
+_libc.strlen.restype = ctypes.c_size_t
+_libc.strlen.argtypes = [ctypes.c_void_p]
+_decode_ascii = ctypes.pythonapi.PyUnicode_DecodeASCII
+_decode_ascii.restype = ctypes.py_object
+_decode_ascii.argtypes = [ctypes.c_void_p, ctypes.c_ssize_t, ctypes.c_char_p]
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libfastfib_ref.so")
@@ -104,7 +111,8 @@ class _Lib:
     def to_string(self, a) -> str:
         a, pa, na = _arr(a)
         ptr = getattr(self.lib, f"{self.prefix}to_string")(pa, na)
-        s = ctypes.string_at(ptr).decode()
+        # one pass from the C string to a str, as fastfib_b200.to_decimal does
+        s = _decode_ascii(ptr, _libc.strlen(ptr), None)
         getattr(self.lib, f"{self.prefix}free")(ptr)
         return s
 
