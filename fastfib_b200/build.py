@@ -3,7 +3,8 @@ host C surface with gcc, linked into one shared library next to this file.
 
     python -m fastfib_b200.build        (or fastfib_b200.build.build())
 
-Objects go to fastfib_b200/_build/.  Only files whose sources changed are
+Objects go to fastfib_b200/_build/; the command line fastfib_b200/fastfib
+links against the library.  Only files whose sources changed are
 recompiled (header changes rebuild everything).
 """
 from __future__ import annotations
@@ -19,6 +20,7 @@ CSRC = os.path.join(PKG, "csrc")
 INC = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libfastfib_b200.so")
+CLI = os.path.join(PKG, "fastfib")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 CC = os.environ.get("CC", "gcc")
@@ -64,6 +66,12 @@ def build(verbose: bool = False) -> str:
         objs.append(obj)
     if _newer(objs, LIB):
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs])
+    # the command line (fastfib [n] [--print]) over the library's Big surface
+    cli_src = os.path.join(CSRC, "cli", "fastfib_cli.c")
+    if _newer([cli_src, LIB, *headers], CLI):
+        if verbose:
+            print("gcc", os.path.basename(cli_src))
+        _run([CC, *CFLAGS, cli_src, "-o", CLI, f"-L{PKG}", "-lfastfib_b200", "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 
