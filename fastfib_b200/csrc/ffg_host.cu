@@ -1191,11 +1191,27 @@ static void mlp_features(uint64_t bits_a, uint64_t bits_b, int square, float *f)
 // product, then per product the method of least predicted cost among those
 // whose plan exists (the forced lengths within the cap).  Without a model,
 // and for products the reference splits, the plain thresholds.
+// The learned choice is a function of (bit lengths, squaring, transform cap)
+// under the installed model: kept per shape, so a batch whose shapes were
+// seen before needs no cost-model round trip (upload, inference, copy back,
+// synchronize) before its first launch.  Cleared when the model changes.
+struct LearnedKey {
+    uint64_t ba, bb, cap;
+    int sq;
+    bool operator<(const LearnedKey &o) const { return std::tie(ba, bb, cap, sq) < std::tie(o.ba, o.bb, o.cap, o.sq); }
+};
+static std::map<LearnedKey, int> g_learned_memo;
+static const size_t kLearnedMemoMax = 1 << 20;
+
 static int learned_resolve(const uint64_t *ba, const uint64_t *bb, const int *sq, int *meth, size_t count,
                            cudaStream_t st) {
     std::vector<size_t> idx;
-    for (size_t i = 0; i < count; i++)
-        if (meth[i] == FFG_M_LEARNED) idx.push_back(i);
+    for (size_t i = 0; i < count; i++) {
+        if (meth[i] != FFG_M_LEARNED) continue;
+        auto it = g_learned_memo.find(LearnedKey{ba[i], bb[i], (uint64_t)g.max_L, sq[i] ? 1 : 0});
+        if (it != g_learned_memo.end()) meth[i] = it->second;
+        else idx.push_back(i);
+    }
     if (idx.empty()) return FFG_OK;
     float *model = mlp_device();
     if (!model) {
@@ -1235,6 +1251,8 @@ static int learned_resolve(const uint64_t *ba, const uint64_t *bb, const int *sq
         }
         meth[i] = best;
     }
+    if (g_learned_memo.size() + idx.size() > kLearnedMemoMax) g_learned_memo.clear();
+    for (size_t i : idx) g_learned_memo[LearnedKey{ba[i], bb[i], (uint64_t)g.max_L, sq[i] ? 1 : 0}] = meth[i];
     return FFG_OK;
 }
 
@@ -1930,6 +1948,7 @@ extern "C" int ffg_mlp_predict(const float *params, const float *X, size_t n, fl
 
 extern "C" int ffg_mlp_set(const float *params) {
     std::lock_guard<std::recursive_mutex> lk(g_mu);
+    g_learned_memo.clear();
     if (!params) {
         g_mlp_host.clear();
         return FFG_OK;
