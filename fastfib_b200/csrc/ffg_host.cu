@@ -24,6 +24,8 @@ static const uint32_t kP[3] = {2113929217u, 2013265921u, 1811939329u}; // src/nt
 static const uint32_t kG[3] = {5u, 31u, 13u};
 static int kMaxLg = 25; // NTT_MAX_LG (src/common.h:46-48); ffg_set_max_lg lowers it like -DNTT_MAX_LG
 static const uint32_t kSmallMaxL = 4096;  // one-CTA transform up to this length for a single product
+// The cost model's "kernel kind" feature keeps the bound it was trained with.
+static const uint32_t kFeatureSmallL = 4096;
 static const int kR3TabLg = 13;           // radix-3 tables cover R = 3 2^n, n < 13
 // Doubling steps whose operands have at most this many limbs square by
 // schoolbook (one launch for the pair) instead of the NTT (transform + CRT):
@@ -1184,7 +1186,7 @@ static void mlp_features(uint64_t bits_a, uint64_t bits_b, int square, float *f)
     f[4] = pl.r3 ? 1.f : 0.f;
     f[5] = (float)(std::log2((double)Lp2) / 26.0);
     f[6] = (float)(std::log2((double)Lr3) / 26.0);
-    f[7] = pl.split || pl.L > kSmallMaxL ? 1.f : 0.f;
+    f[7] = pl.split || pl.L > kFeatureSmallL ? 1.f : 0.f;
 }
 
 // Resolves FFG_M_LEARNED in meth[]: one inference launch over every such
@@ -1263,11 +1265,29 @@ struct GroupKey {
     }
 };
 
+static const uint64_t kBatchSmallMaxL = 16384; // longest line one CTA holds (FFG_LINE_LG)
+static const size_t kBatchSmallMin = 64;       // products of one plan (a decimal level has hundreds)
+
 // Runs a batch: one schoolbook launch for every schoolbook product, then per
 // group of products sharing an NTT plan one transform launch set and one CRT
 // launch; split products one by one.  Job records go to the device in one
 // copy.
 static int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capture = nullptr) {
+    // Many products of one four-step plan up to L = kBatchSmallMaxL: one CTA
+    // per (product, prime) holding the whole transform beats three launches
+    // once the group alone fills the GPU (a doubling step's pair does not).
+    {
+        std::map<GroupKey, size_t> count;
+        for (const BJob &J : jobs)
+            if (!J.school && !J.pl.split && J.pl.kernel == 1 && J.pl.L <= kBatchSmallMaxL)
+                count[GroupKey{1, J.pl.lg, J.pl.r3, J.pl.width, J.pl.row_lg, (uint32_t)J.square}]++;
+        for (BJob &J : jobs)
+            if (!J.school && !J.pl.split && J.pl.kernel == 1 && J.pl.L <= kBatchSmallMaxL &&
+                count[GroupKey{1, J.pl.lg, J.pl.r3, J.pl.width, J.pl.row_lg, (uint32_t)J.square}] >= kBatchSmallMin) {
+                J.pl.kernel = 0;
+                J.pl.row_lg = 0;
+            }
+    }
     std::vector<SchoolJob> sj;
     std::map<GroupKey, std::vector<size_t>> groups;
     std::vector<size_t> splits;

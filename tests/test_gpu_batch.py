@@ -94,3 +94,30 @@ def test_device_batch(ff):
         out = keep[3 * i + 2].cpu().numpy().view(np.uint64)
         x = limbs_to_int(a)
         assert limbs_to_int(out) == x * (x if j["square"] else limbs_to_int(b))
+
+
+@pytest.mark.parametrize("L", [6144, 8192, 12288, 16384])
+@pytest.mark.parametrize("square", [True, False])
+def test_large_group_one_cta(ff, L, square):
+    """Groups of at least 64 products sharing a four-step plan of length up to
+    16384 run one CTA per (product, prime) with the whole transform in
+    shared memory: 64 products of each length (both length families,
+    squares and distinct), against Python integers."""
+    rng = np.random.default_rng(L + square)
+    coeffs = int(0.85 * L)
+    pairs = []
+    for _ in range(64):
+        if square:
+            a = rng.integers(0, 2**64, size=(coeffs * 32 // 2 + 63) // 64, dtype=np.uint64)
+            a[-1] |= np.uint64(1 << 63)
+            pairs.append((a, None))
+        else:
+            a = rng.integers(0, 2**64, size=(coeffs * 32 // 3 + 63) // 64, dtype=np.uint64)
+            b = rng.integers(0, 2**64, size=(2 * coeffs * 32 // 3 + 63) // 64, dtype=np.uint64)
+            a[-1] |= np.uint64(1 << 63)
+            b[-1] |= np.uint64(1 << 63)
+            pairs.append((a, b))
+    plan = ff.plan(64 * pairs[0][0].size, 64 * (pairs[0][0] if square else pairs[0][1]).size, square)
+    assert plan["L"] == L and plan["kernel"] == 1, plan
+    got = ff.mul_batch(pairs)
+    assert [limbs_to_int(g) for g in got] == exact(pairs)
