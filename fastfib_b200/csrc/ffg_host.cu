@@ -92,6 +92,9 @@ static void dec_free();
 // belongs to the allocation-free multiply.
 constexpr uint32_t kTicketsLive = 1u << 16, kTicketsCapture = 1u << 13;
 static uint32_t *g_tickets = nullptr;
+// The decimal host entry point's device copy of its number, kept between calls.
+static uint64_t *g_dec_in = nullptr;
+static size_t g_dec_in_cap = 0;
 static uint32_t g_ticket_live = 0, g_ticket_cap = 0;
 static bool g_capturing = false, g_capture_starved = false;
 
@@ -1603,6 +1606,9 @@ extern "C" void ffg_shutdown(void) {
     g.tables = nullptr;
     if (g_mlp) cudaFree(g_mlp);
     g_mlp = nullptr;
+    if (g_dec_in) cudaFree(g_dec_in);
+    g_dec_in = nullptr;
+    g_dec_in_cap = 0;
     if (g_tickets) cudaFree(g_tickets);
     g_tickets = nullptr;
     dec_free();
@@ -2438,16 +2444,27 @@ extern "C" int ffg_to_decimal_host(const uint64_t *x, size_t nx, char **out, siz
     if (nx == 1 && x[0] == 0) return FFG_OK;
     CK(cudaStreamSynchronize(g.stream));
     arena_reset();
-    // the number gets its own allocation: dec_device resets the arena
-    uint64_t *dx = nullptr;
-    CK(cudaMalloc(&dx, nx * 8));
-    cudaError_t e = cudaMemcpy(dx, x, nx * 8, cudaMemcpyHostToDevice);
+    // the number gets a buffer of its own, kept between calls (dec_device
+    // resets the arena), filled through a pinned staging copy
+    if (g_dec_in_cap < nx) {
+        if (g_dec_in) cudaFree(g_dec_in);
+        g_dec_in = nullptr;
+        g_dec_in_cap = 0;
+        CK(cudaMalloc(&g_dec_in, nx * 8));
+        g_dec_in_cap = nx;
+    }
+    uint64_t *stage = (uint64_t *)pinned_get(nx * 8);
+    if (!stage) return fail(FFG_E_NOMEM, "pinned staging: %zu bytes", nx * 8);
+    memcpy(stage, x, nx * 8);
+    cudaError_t e = cudaMemcpyAsync(g_dec_in, stage, nx * 8, cudaMemcpyHostToDevice, g.stream);
     if (e) {
-        cudaFree(dx);
+        cudaStreamSynchronize(g.stream);
+        pinned_release(stage);
         return fail(FFG_E_CUDA, "decimal upload: %s", cudaGetErrorString(e));
     }
-    rc = ffg_to_decimal_device(dx, nx, out, nout, done);
-    cudaFree(dx);
+    rc = ffg_to_decimal_device(g_dec_in, nx, out, nout, done); // synchronizes before returning
+    cudaStreamSynchronize(g.stream);
+    pinned_release(stage);
     return rc;
 }
 
