@@ -275,7 +275,7 @@ def to_decimal(a, device_ptr: int = 0, n: int = 0):
     if not done.value:
         return None, False
     s = _ascii_str(out.value, nout.value)
-    ctypes.CDLL(None).free(out)
+    lib().ffg_free(out)
     return s, True
 
 

@@ -2394,11 +2394,17 @@ static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, s
             *fallback = true;
             return FFG_OK;
         }
+    // the digits land in a pooled pinned buffer (one DMA at full speed, no
+    // fresh pages to fault in); the caller returns it with ffg_free
     const uint64_t nd = total - first;
-    char *h = (char *)malloc(nd + 1);
+    char *h = (char *)pinned_get(nd + 1);
     if (!h) return fail(FFG_E_NOMEM, "host digits");
-    CK(cudaMemcpyAsync(h, dd + first, nd, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    e = cudaMemcpyAsync(h, dd + first, nd, cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaStreamSynchronize(st);
+    if (e) {
+        pinned_release(h);
+        return fail(FFG_E_CUDA, "digits download: %s", cudaGetErrorString(e));
+    }
     h[nd] = 0;
     *out = h;
     *nout = nd;

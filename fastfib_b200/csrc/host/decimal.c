@@ -143,7 +143,12 @@ char *big_to_string(const Big *a) {
         size_t n = 0;
         int done = 0;
         if (ffg_to_decimal_host(a->d, a->n, &s, &n, &done)) ff_gpu_failed("decimal conversion", ffg_last_error());
-        if (done) return s;
+        if (done) { /* big_to_string's result is the caller's to free() */
+            char *m = xmalloc(n + 1);
+            memcpy(m, s, n + 1);
+            ffg_free(s);
+            return m;
+        }
         /* declined (a correction out of range): the level-by-level path below */
     }
     DecCtx *c = xmalloc(sizeof(DecCtx));

@@ -149,8 +149,8 @@ int ffg_time_batch(ffg_job *jobs, size_t count, int reps, double *ms);
 /* Decimal digits (big_to_string, src/decimal.c:229-281) of a number on the
    device (x: device pointer) or on the host (x: host pointer), converted on
    the device level by level: every level's Barrett products in shared
-   launches.  *out is a malloc'd NUL-terminated string of *nout digits (free
-   with free()).  *done = 0 when the device path declines -- numbers below
+   launches.  *out is a NUL-terminated string of *nout digits in one of this
+   layer's pooled pinned buffers: return it with ffg_free().  *done = 0 when the device path declines -- numbers below
    about 10^4900 and a quotient correction out of range (which its bounds
    rule out) --
    and the caller converts another way (big_to_string then uses its host
