@@ -1207,9 +1207,51 @@ struct LearnedKey {
 };
 static std::map<LearnedKey, int> g_learned_memo;
 static const size_t kLearnedMemoMax = 1 << 20;
+// The last batch's shapes (a hash and the shapes themselves) and its
+// resolved methods: a batch repeated call after call is resolved by one
+// comparison pass, with no per-product lookups before its first launch.
+static uint64_t g_learned_sig = 0, g_learned_cap = 0;
+static std::vector<uint64_t> g_learned_shapes;
+static std::vector<int> g_learned_meth;
+
+static int learned_resolve_shapes(const uint64_t *ba, const uint64_t *bb, const int *sq, int *meth, size_t count,
+                                  cudaStream_t st);
 
 static int learned_resolve(const uint64_t *ba, const uint64_t *bb, const int *sq, int *meth, size_t count,
                            cudaStream_t st) {
+    uint64_t h = 1469598103934665603ull ^ (uint64_t)g.max_L; // FNV-1a over the shapes and methods asked for
+    for (size_t i = 0; i < count; i++) {
+        h = (h ^ ba[i]) * 1099511628211ull;
+        h = (h ^ bb[i]) * 1099511628211ull;
+        h = (h ^ (uint64_t)(sq[i] ? 1 : 0) ^ ((uint64_t)(uint32_t)meth[i] << 8)) * 1099511628211ull;
+    }
+    if (h == g_learned_sig && g_learned_cap == (uint64_t)g.max_L && g_learned_meth.size() == count) {
+        bool same = true;
+        for (size_t i = 0; i < count && same; i++)
+            same = g_learned_shapes[3 * i] == ba[i] && g_learned_shapes[3 * i + 1] == bb[i] &&
+                   g_learned_shapes[3 * i + 2] == (((uint64_t)(uint32_t)meth[i] << 1) | (sq[i] ? 1u : 0u));
+        if (same) {
+            for (size_t i = 0; i < count; i++) meth[i] = g_learned_meth[i];
+            return FFG_OK;
+        }
+    }
+    g_learned_shapes.resize(3 * count);
+    for (size_t i = 0; i < count; i++) {
+        g_learned_shapes[3 * i] = ba[i];
+        g_learned_shapes[3 * i + 1] = bb[i];
+        g_learned_shapes[3 * i + 2] = ((uint64_t)(uint32_t)meth[i] << 1) | (sq[i] ? 1u : 0u);
+    }
+    g_learned_sig = 0;
+    const int rc = learned_resolve_shapes(ba, bb, sq, meth, count, st);
+    if (rc) return rc;
+    g_learned_meth.assign(meth, meth + count);
+    g_learned_sig = h;
+    g_learned_cap = (uint64_t)g.max_L;
+    return FFG_OK;
+}
+
+static int learned_resolve_shapes(const uint64_t *ba, const uint64_t *bb, const int *sq, int *meth, size_t count,
+                                  cudaStream_t st) {
     std::vector<size_t> idx;
     for (size_t i = 0; i < count; i++) {
         if (meth[i] != FFG_M_LEARNED) continue;
@@ -1975,6 +2017,8 @@ extern "C" int ffg_mlp_predict(const float *params, const float *X, size_t n, fl
 extern "C" int ffg_mlp_set(const float *params) {
     std::lock_guard<std::recursive_mutex> lk(g_mu);
     g_learned_memo.clear();
+    g_learned_sig = 0;
+    g_learned_meth.clear();
     if (!params) {
         g_mlp_host.clear();
         return FFG_OK;
