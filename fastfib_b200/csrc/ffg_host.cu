@@ -28,9 +28,11 @@ static const uint32_t kSmallMaxL = 4096;  // one-CTA transform up to this length
 static const uint32_t kFeatureSmallL = 4096;
 static const int kR3TabLg = 13;           // radix-3 tables cover R = 3 2^n, n < 13
 // Doubling steps whose operands have at most this many limbs square by
-// schoolbook (one launch for the pair) instead of the NTT (transform + CRT):
-// at these sizes both are latency-bound and the schoolbook takes one launch.
-static const uint64_t kChainSchoolLimbs = 256;
+// schoolbook (k_school_sq_pair, one launch for the pair) instead of the NTT
+// (transform + CRT): at these sizes both are latency-bound.  Measured on the
+// F(10^8) chain: 256 limbs 0.947 ms, 512 0.939, 768 0.939 (and 8 us less
+// than 256 on chains of n ~ 10^5).
+static const uint64_t kChainSchoolLimbs = 768;
 
 // ------------------------------------------------------------ host modmath
 
