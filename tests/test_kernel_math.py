@@ -101,3 +101,76 @@ def test_school_square_columns():
         a = [rng.getrandbits(64) if rng.random() < 0.8 else M64 for _ in range(n)]
         x = sum(v << (64 * i) for i, v in enumerate(a))
         assert sum(square_column(a, j) << (64 * j) for j in range(2 * n + 1)) == x * x
+
+
+def settle(out, cta_limbs, maps, walk=8, long_max=64):
+    """settle_cta (ffg_ripple.cuh) restated: the carry into every CTA from the
+    composed maps, each carried in by a bounded walk of `walk` limbs; carries
+    still running go to a list finished 'by the block' (first limb that is
+    not 2^64 - 1 gains 1, the ones before it become 0); past `long_max`
+    entries the walk simply continues."""
+    ncta = len(maps)
+    carry, pending = 0, []
+    for q in range(ncta):
+        if carry:
+            j, end = q * cta_limbs, min(len(out), (q + 1) * cta_limbs)
+            running = True
+            for _ in range(walk):
+                if j >= end:
+                    break
+                out[j] = (out[j] + 1) & M64
+                j += 1
+                if out[j - 1] != 0:
+                    running = False
+                    break
+            if running and j < end:
+                if len(pending) < long_max:
+                    pending.append((j, end))
+                else:
+                    while j < end:
+                        out[j] = (out[j] + 1) & M64
+                        j += 1
+                        if out[j - 1] != 0:
+                            break
+        carry = (maps[q] >> carry) & 1  # bit c: carry out for carry in c
+    for j0, end in pending:
+        first = next((j for j in range(j0, end) if out[j] != M64), None)
+        for j in range(j0, end if first is None else first):
+            out[j] = 0
+        if first is not None:
+            out[first] += 1
+
+
+def test_settle_long_carries():
+    rng = random.Random(7)
+    for trial in range(300):
+        cta, ncta = rng.choice([4, 8, 32]), rng.randint(1, 12)
+        n = cta * ncta - rng.randint(0, cta - 1)
+        # per-CTA limbs as each CTA leaves them (no carry in), with runs of 2^64 - 1
+        limbs = []
+        for _ in range(n):
+            r = rng.random()
+            limbs.append(M64 if r < 0.6 else (0 if r < 0.65 else rng.getrandbits(64)))
+        # a CTA's own carry out (c_in = 0); a CTA whose limbs all propagate
+        # (2^64 - 1) generates none: a group's generate and propagate exclude each other
+        carries_out = []
+        for q in range(ncta):
+            seg = limbs[q * cta:min(n, (q + 1) * cta)]
+            carries_out.append(rng.random() < 0.5 and not all(v == M64 for v in seg))
+        # the true value: each CTA's limbs plus its own carry out at the next CTA's start
+        want = sum(v << (64 * i) for i, v in enumerate(limbs))
+        for q in range(ncta - 1):
+            if carries_out[q]:
+                want += 1 << (64 * (q + 1) * cta)
+        want &= (1 << (64 * n)) - 1
+        # maps: carry out for c_in = 0 and 1 (c_in = 1 wraps the CTA when every limb is 2^64 - 1)
+        maps = []
+        for q in range(ncta):
+            seg = limbs[q * cta:min(n, (q + 1) * cta)]
+            all_ones = all(v == M64 for v in seg)
+            c0 = int(carries_out[q])
+            c1 = 1 if (c0 or all_ones) else 0
+            maps.append(c0 | (c1 << 1))
+        out = list(limbs)
+        settle(out, cta, maps, walk=rng.choice([1, 2, 8]), long_max=rng.choice([1, 64]))
+        assert sum(v << (64 * i) for i, v in enumerate(out)) == want, trial
