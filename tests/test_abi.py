@@ -61,3 +61,33 @@ def test_gpu_calls_fail_loudly_without_gpu(ff):
         pass
     with pytest.raises(ff.FfgError):
         ff.mul(np.ones(300, dtype=np.uint64))
+
+
+def test_plan_select_sweep(ff, oracle):
+    """The width / length / split choice of big_mul_ntt (src/mul_ntt.c:97-118,
+    src/mul_split.c:150-177) on 1500 seeded shapes, squares and distinct,
+    log-uniform 2^6..2^28 bits, under transform caps 2^10, 2^16, 2^22 and
+    2^25: every field the oracle restatement gives, the split's included."""
+    import math
+    import random
+    rng = random.Random(23)
+    saved = oracle.ntt_max_L()
+    try:
+        for cap_lg in (10, 16, 22, 25):
+            oracle.set_ntt_max_L(1 << cap_lg)
+            ff.lib().ffg_set_ntt_max_L(1 << cap_lg)
+            for _ in range(375):
+                ba = int(2 ** rng.uniform(6, 28))
+                sq = rng.random() < 0.3
+                bb = ba if sq else int(2 ** min(28.0, max(6.0, math.log2(ba) + rng.uniform(-4, 4))))
+                p = ff.plan(ba, bb, sq)
+                o = oracle.plan(ba, bb, sq)
+                assert (p["split"], p["width"], p["L"], p["lg"], p["r3"]) == (o.split, o.width, o.L, o.lg, o.r3), \
+                    (cap_lg, ba, bb, sq, p)
+                if o.split:
+                    assert (p["ka"], p["kb"], p["Lbig"]) == (o.ka, o.kb, o.Lbig), (cap_lg, ba, bb, sq)
+                else:
+                    assert p["conv"] == o.conv
+    finally:
+        oracle.set_ntt_max_L(saved)
+        ff.lib().ffg_set_ntt_max_L(saved)
