@@ -163,3 +163,19 @@ def test_oracle_against_reference(oracle, reference):
         assert np.array_equal(f, reference.fibonacci(n))
         if n < 200000:
             assert oracle.to_string(f) == reference.to_string(f)
+
+
+@pytest.mark.parametrize("lg", [4, 6, 8])
+def test_split_tiny_caps(oracle, lg):
+    """The split multiply under transform caps of 2^4..2^8 (pieces as short as
+    16 coefficients), as the GPU's test_split_tiny_pieces runs it."""
+    saved = oracle.ntt_max_L()
+    try:
+        oracle.set_ntt_max_L(1 << lg)
+        rng = random.Random(200 + lg)
+        for na, nb in ((40, 40), (100, 37), (300, 300)):
+            x, y = rng.getrandbits(64 * na), rng.getrandbits(64 * nb)
+            assert limbs_to_int(oracle.mul_ntt(int_to_limbs(x), int_to_limbs(y))) == x * y, (lg, na, nb)
+            assert limbs_to_int(oracle.mul_ntt(int_to_limbs(x))) == x * x, (lg, na)
+    finally:
+        oracle.set_ntt_max_L(saved)
