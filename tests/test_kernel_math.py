@@ -174,3 +174,29 @@ def test_settle_long_carries():
         out = list(limbs)
         settle(out, cta, maps, walk=rng.choice([1, 2, 8]), long_max=rng.choice([1, 64]))
         assert sum(v << (64 * i) for i, v in enumerate(out)) == want, trial
+
+
+def test_fingerprint_runs():
+    """k_fp_partial (ffg_fingerprint.cu) restated: thread t reduces limbs
+    [t*per, (t+1)*per) by Horner's rule from the top with 2^64 mod p, weights
+    the run by (2^64)^(first limb) mod p, and the runs' residues sum to
+    x mod p; runs past the end are empty."""
+    primes = (18446744073709551557, 18446744073709551533, 9223372036854775783, 4611686018427387847)
+    rng = random.Random(5)
+    for n in (0, 1, 2, 7, 64, 1000, 4097):
+        limbs = [rng.getrandbits(64) if rng.random() < 0.9 else M64 for _ in range(n)]
+        x = sum(v << (64 * i) for i, v in enumerate(limbs))
+        for nthreads in (1, 3, 256, 5000):
+            per = (n + nthreads - 1) // nthreads
+            for p in primes:
+                r64 = (1 << 64) % p
+                total = 0
+                for t in range(nthreads):
+                    i0, i1 = min(t * per, n), min(t * per + per, n)
+                    h = 0
+                    for i in range(i1 - 1, i0 - 1, -1):
+                        h = (h * r64 + limbs[i]) % p
+                    if h:
+                        h = h * pow(r64, i0, p) % p
+                    total = (total + h) % p
+                assert total == x % p, (n, nthreads, p)
