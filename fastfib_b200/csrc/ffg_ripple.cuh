@@ -98,10 +98,12 @@ FFG_DEV_INLINE uint32_t cta_resolve(uint64_t *lo, const uint32_t *hi, uint32_t h
 // block-wide scan of those composites gives the carry into every run (carry
 // 0 into the first CTA), and each thread walks its run again adding the
 // carry into the CTAs that receive one: a carry stops at the first limb that
-// does not wrap, almost always the first.  A carry still running after
-// kSettleWalk limbs (a CTA whose limbs are mostly 2^64 - 1, which Barrett and
-// Newton combinations produce) is finished by the whole block afterwards,
-// 256 limbs at a time, so no thread walks thousands of dependent loads.
+// does not wrap, almost always the first.  A CTA whose map is the identity
+// has every limb 2^64 - 1 (Barrett and Newton combinations produce long such
+// runs): the carry zeroes it with stores alone.  A carry still running after
+// kSettleWalk limbs of any other CTA is finished by the whole block
+// afterwards, 256 limbs at a time, so no thread walks thousands of dependent
+// loads.
 // Maps and limbs written by other CTAs are read through L2.
 constexpr uint32_t kSettleWalk = 8;
 constexpr uint32_t kSettleLong = 64;
@@ -132,7 +134,13 @@ FFG_DEV_INLINE void settle_cta(uint64_t *out, uint64_t nlimbs, uint32_t cta_limb
     const uint32_t before = warp ? map_then(wpre[warp - 1], exc) : exc;
     uint32_t carry = map_apply(before, 0);
     for (uint32_t q = q0; q < q1; q++) {
-        if (carry) {
+        const uint32_t mq = __ldcg(&maps[q]);
+        if (carry && mq == 2u) {
+            // the identity map: every limb of the CTA is 2^64 - 1, so the
+            // carry turns them all to 0 and goes on (stores only, no search)
+            const uint64_t end = min(nlimbs, (uint64_t)(q + 1) * cta_limbs);
+            for (uint64_t j = (uint64_t)q * cta_limbs; j < end; j++) out[j] = 0;
+        } else if (carry) {
             const uint64_t end = min(nlimbs, (uint64_t)(q + 1) * cta_limbs);
             uint64_t j = (uint64_t)q * cta_limbs;
             bool running = true;
@@ -158,7 +166,7 @@ FFG_DEV_INLINE void settle_cta(uint64_t *out, uint64_t nlimbs, uint32_t cta_limb
                 }
             }
         }
-        carry = map_apply(__ldcg(&maps[q]), carry);
+        carry = map_apply(mq, carry);
     }
     __syncthreads();
     // the long carries, one at a time by the whole block: limbs before the

@@ -105,14 +105,18 @@ def test_school_square_columns():
 
 def settle(out, cta_limbs, maps, walk=8, long_max=64):
     """settle_cta (ffg_ripple.cuh) restated: the carry into every CTA from the
-    composed maps, each carried in by a bounded walk of `walk` limbs; carries
+    composed maps; a CTA with the identity map zeroed outright, any other
+    carried into by a bounded walk of `walk` limbs; carries
     still running go to a list finished 'by the block' (first limb that is
     not 2^64 - 1 gains 1, the ones before it become 0); past `long_max`
     entries the walk simply continues."""
     ncta = len(maps)
     carry, pending = 0, []
     for q in range(ncta):
-        if carry:
+        if carry and maps[q] == 2:  # the identity map: every limb 2^64 - 1, all wrap to 0
+            for j in range(q * cta_limbs, min(len(out), (q + 1) * cta_limbs)):
+                out[j] = 0
+        elif carry:
             j, end = q * cta_limbs, min(len(out), (q + 1) * cta_limbs)
             running = True
             for _ in range(walk):
@@ -150,7 +154,7 @@ def test_settle_long_carries():
         limbs = []
         for _ in range(n):
             r = rng.random()
-            limbs.append(M64 if r < 0.6 else (0 if r < 0.65 else rng.getrandbits(64)))
+            limbs.append(M64 if r < 0.8 else (0 if r < 0.83 else rng.getrandbits(64)))
         # a CTA's own carry out (c_in = 0); a CTA whose limbs all propagate
         # (2^64 - 1) generates none: a group's generate and propagate exclude each other
         carries_out = []
