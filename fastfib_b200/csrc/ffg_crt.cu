@@ -179,14 +179,20 @@ static size_t crt_smem() {
     return (CRT_COEF + CRT_HALO_MAX) * (8 + 4) + CRT_NL_MAX * (8 + 4) + 3 * (CRT_NL_MAX / 32) * 4;
 }
 
+static bool g_crt_configured = false;
+
+cudaError_t crt_kernel_load() {
+    if (g_crt_configured) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_crt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)crt_smem());
+    if (e) return e;
+    g_crt_configured = true;
+    return cudaSuccess;
+}
+
 cudaError_t launch_crt(const Primes3 &P3, const CrtJob &J, cudaStream_t st) {
     (void)P3;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_crt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)crt_smem());
-        if (e) return e;
-        configured = true;
-    }
+    cudaError_t e0 = crt_kernel_load();
+    if (e0) return e0;
     const uint32_t ncta = crt_ctas(J.nlimbs, J.width);
     prof_begin(PK_CRT, st);
     k_crt<<<ncta, CRT_THREADS, crt_smem(), st>>>(garner_const(), J);

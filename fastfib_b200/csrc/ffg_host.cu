@@ -1499,10 +1499,21 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capt
 
 using namespace ffg;
 
+static int noalloc_address(int dev, void **addr);
+
 extern "C" int ffg_init(size_t max_limbs) {
     std::lock_guard<std::recursive_mutex> lk(g_mu);
     int rc = ensure_ready();
     if (rc) return rc;
+    // the allocation-free multiply's scratch address, looked up now: the
+    // lookup loads the module holding the array (which places it on the
+    // device), so that entry point allocates nothing even on its first call
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    void *scratch = nullptr;
+    if ((rc = noalloc_address(dev, &scratch))) return rc;
+    CK(ntt_kernels_load()); // and the kernels it launches, for the same reason
+    CK(crt_kernel_load());
     size_t L = 16;
     while (L < 2 * max_limbs && L < ((size_t)1 << kMaxLg)) L <<= 1;
     if (L > g.max_L) g.max_L = L;
@@ -1639,6 +1650,8 @@ extern "C" void ffg_free(void *p) {
     if (!ffg_release(p)) free(p);
 }
 
+static void *g_noalloc_addr[64]; // the allocation-free scratch's device address, per device
+
 extern "C" void ffg_shutdown(void) {
     std::lock_guard<std::recursive_mutex> lk(g_mu);
     if (!g.ready) return;
@@ -1662,26 +1675,26 @@ extern "C" void ffg_shutdown(void) {
     cudaEventDestroy(g.ev1);
     cudaStreamDestroy(g.stream);
     g.ready = false;
+    for (auto &a : g_noalloc_addr) a = nullptr; // looked up again by the next ffg_init
 }
 
 // ======================================================= allocation-free multiply
 //
 // ffg_mul_device_noalloc: the NTT product of ffg_mul_device for callers that
-// must not allocate device memory once they are running -- code executing
-// while a CUDA graph is being captured on its stream, a framework that owns
-// all device memory through its own allocator, or a latency-critical path
-// that cannot afford a cudaMalloc (and the device-wide synchronization it may
-// imply).  Its scratch (the residue arrays, the job record and the CRT's carry
+// must not allocate device memory once they are running -- a host program
+// whose device memory is all owned by another allocator (a framework's
+// caching allocator, a fixed budget handed out at start-up), or a
+// latency-critical path that cannot afford a cudaMalloc (and the device-wide
+// synchronization it may imply).  Its scratch (the residue arrays, the job record and the CRT's carry
 // maps) lives in the fixed array below, which every GPU that loads this
 // library holds until the process exits; products whose scratch would not fit
 // are rejected with FFG_E_RANGE.  The device tables are built once by
-// ffg_init, which the caller runs during its own set-up; this entry point
-// itself calls no cudaMalloc, cudaFree or other allocating routine.
+// ffg_init, which the caller runs during its own set-up and which also looks
+// up the array's device address and loads the kernels used here; this entry
+// point itself calls no cudaMalloc, cudaFree or other allocating routine.
 
 static constexpr size_t kNoAllocBytes = (size_t)8 << 20; // 8 MiB per device
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
-static void *g_noalloc_addr[64]; // the array's device address, per device
-
 // Host code may not use g_noalloc_scratch's name as an address (it is a host
 // stand-in); the device address comes from cudaGetSymbolAddress, looked up
 // once per device with that device current.

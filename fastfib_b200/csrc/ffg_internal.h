@@ -223,6 +223,10 @@ cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_
 uint32_t lin_ctas(uint64_t len);                    // CTAs of one linear pass
 
 cudaError_t set_line_consts(const LineConsts &h); // once, before any transform
+// Load (and configure) the kernels of one product -- the transforms and the
+// plain CRT -- during set-up, so a later first launch loads no module code.
+cudaError_t ntt_kernels_load();
+cudaError_t crt_kernel_load();
 cudaError_t launch_conv_small(const Primes3 &P3, const ConvJobs &jobs, uint32_t njobs, uint32_t maxL,
                               bool any_distinct, cudaStream_t st, double bytes);
 cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t njobs,

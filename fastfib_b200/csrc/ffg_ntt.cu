@@ -252,6 +252,8 @@ static cudaError_t smem_optin() {
     return cudaSuccess;
 }
 
+cudaError_t ntt_kernels_load() { return smem_optin(); }
+
 static size_t small_smem_bytes(uint32_t L, bool square) {
     return (size_t)line_stride(L) * (square ? 1 : 2) * sizeof(uint32_t);
 }

@@ -192,17 +192,19 @@ int ffg_get_geometry(uint32_t lg, uint32_t r3, uint32_t *row_lg, uint32_t *wc);
 int ffg_load_tuning(const char *path);
 
 /* No counterpart in the reference.  ffg_mul_device without any device
-   allocation, for callers that cannot allocate once running: code issuing
-   work while a CUDA graph is being captured, frameworks whose allocator owns
-   all device memory, latency-critical paths that cannot take a cudaMalloc.
-   Scratch comes from one fixed 8 MiB array per GPU, held by every GPU that
-   loads the library until the process exits; products whose scratch does not
-   fit (transform lengths above 2^19 for a square or 2^18 for two distinct
-   operands, about 130 000 and 65 000 limbs per operand), or that need the
-   split multiply, return FFG_E_RANGE with the bytes needed in the message.
-   ffg_init must have run first (it builds the device tables; run it during
-   set-up).  The first call on a device looks the array's address up; make
-   that first call before any stream capture.  All calls share the one array:
+   allocation, for callers that cannot allocate once running: host programs
+   whose device memory is all owned by another allocator (a framework's
+   caching allocator, a fixed budget handed out at start-up) and
+   latency-critical paths that cannot take a cudaMalloc and the device-wide
+   synchronization it may bring.  Scratch comes from one fixed 8 MiB array
+   per GPU, held by every GPU that loads the library until the process exits;
+   products whose scratch does not fit (transform lengths above 2^19 for a
+   square or 2^18 for two distinct operands, about 130 000 and 65 000 limbs
+   per operand), or that need the split multiply, return FFG_E_RANGE with the
+   bytes needed in the message.  ffg_init must have run first: it builds the
+   device tables, looks the array's address up (with the device current) and
+   loads the kernels used here, so the first call allocates nothing either.
+   All calls share the one array, and it keeps the last call's contents:
    calls whose GPU work overlaps (different streams, no ordering between
    them) race and corrupt each other's results. */
 int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b,

@@ -27,7 +27,8 @@ _decode_ascii.argtypes = [ctypes.c_void_p, ctypes.c_ssize_t, ctypes.c_char_p]
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libfastfib_ref.so")
-REF_SRC = "/root/reference"
+# the reference's source tree (read only); FASTFIB_REF overrides the default
+REF_SRC = os.environ.get("FASTFIB_REF", "/root/reference")
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _szp = ctypes.POINTER(ctypes.c_size_t)

@@ -26,7 +26,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+REF = os.environ.get("FASTFIB_REF", "/root/reference")
 sys.path.insert(0, ROOT)
 sys.path.insert(0, REF)
 sys.set_int_max_str_digits(0)

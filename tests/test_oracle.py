@@ -141,7 +141,8 @@ def test_split_forced(oracle):
 
 def test_plan_matches_reference_choice(oracle):
     """The width / length choice of big_mul_ntt at the microbench sizes
-    (SURVEY: 2^14, 2^17, 2^20, 2^22 limbs squared -> L = 2^16, 2^19, 2^22, 2^24 at b = 32)."""
+    (2^14, 2^17, 2^20, 2^22 limbs squared -> L = 2^16, 2^19, 2^22, 2^24 at b = 32, as the
+    reference build picks them)."""
     oracle.ntt_init(1 << 24)
     for lg_limbs, lg_L in ((14, 16), (17, 19), (20, 22), (22, 24)):
         bits = 64 << lg_limbs
