@@ -39,6 +39,9 @@ def build(with_reference: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     if with_reference and os.path.isdir(REF_SRC):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
+        # the reference's harnesses against the library (needs the library built first)
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "fastfib_b200", "libfastfib_b200.so")):
+            subprocess.run(["make", "-s", "-C", HERE, "dropin", f"REF={REF_SRC}"], check=True)
 
 
 def int_to_limbs(x: int) -> np.ndarray:

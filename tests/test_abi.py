@@ -91,3 +91,24 @@ def test_plan_select_sweep(ff, oracle):
     finally:
         oracle.set_ntt_max_L(saved)
         ff.lib().ffg_set_ntt_max_L(saved)
+
+
+def test_small_decimal_on_the_host(ff):
+    """big_to_string below 16384 bits runs on the host (no GPU): every class of
+    the reference's tests/dectest.py that fits -- zero, powers of ten and
+    their neighbours, all-ones, chunk boundaries of 10^9 and 10^19, random
+    numbers of every length up to the limit -- against Python's str."""
+    import random
+
+    from oracle import int_to_limbs
+    rng = random.Random(7)
+    xs = [0, 1, 9, 10, 999999999, 10**9, 10**9 + 1, 2**32 - 1, 2**32, 2**64 - 1, 2**64, 10**19 - 1, 10**19,
+          10**19 + 1, 10**18 * 10**9, 2**16382 + 1, 2**16384 - 1 >> 1]
+    for e in (1, 9, 18, 19, 38, 100, 1000, 2400, 4931):
+        xs += [10**e - 1, 10**e, 10**e + 1]
+    for bits in (1, 31, 32, 33, 63, 64, 65, 127, 128, 129, 1000, 4096, 8191, 8192, 12345, 16383):
+        xs.append(rng.getrandbits(bits) | (1 << (bits - 1)))
+        xs.append((1 << bits) - 1)
+    for x in xs:
+        assert x.bit_length() < 16384
+        assert ff.big_to_string(int_to_limbs(x)) == str(x), x.bit_length()
