@@ -1,0 +1,305 @@
+// The four-step column passes with the column length fixed at compile time,
+// for columns of R = 2^RN words (6 <= RN <= 13).
+//
+// A CTA holds a tile of wc columns x R rows in shared memory, one padded
+// line per column.  The length-R transform of each column is three radix
+// steps (decimation in frequency forward, in time inverse):
+//   A: radix 2^MA at stride R / 2^MA (absent when RN <= 9),
+//   B: radix 2^MB at stride 32,
+//   C: radix 32 at stride 1 (no step twiddles).
+// k_col_fwd2: the first step reads the operand's digits straight from its
+//   limbs (the reference's Src reader, src/ntt_kernels.c:29-74, one digit per
+//   word), step C ends with the four-step twiddle ω_L^(n2 k1) and stores the
+//   residues row-major, as the generic column pass (ffg_ntt.cu k_col_fwd).
+// k_col_inv2: step C^-1 reads the row pass's output straight from global
+//   memory, the last step scales by 2^32 / L and stores (or adds into the
+//   split's residues), as k_col_inv.
+// Each step maps thread slots p = threadIdx.x + 256 k to (column p mod wc,
+// group p / wc), so a warp's global accesses cover min(wc, 32) consecutive
+// words of each row it touches, and consecutive lines start 32 / min(wc, 32)
+// banks apart, so no shared access has a bank conflict.
+#include "ffg_internal.h"
+#include "ffg_lines.cuh"
+
+namespace ffg {
+
+__host__ __device__ constexpr int brev5(int u) { return ((u & 1) << 4) | ((u & 2) << 2) | (u & 4) | ((u & 8) >> 2) | ((u & 16) >> 4); }
+
+template <int RN> struct ColShape;
+template <> struct ColShape<6> { static constexpr int MA = 0, MB = 1; };
+template <> struct ColShape<7> { static constexpr int MA = 0, MB = 2; };
+template <> struct ColShape<8> { static constexpr int MA = 0, MB = 3; };
+template <> struct ColShape<9> { static constexpr int MA = 0, MB = 4; };
+template <> struct ColShape<10> { static constexpr int MA = 2, MB = 3; };
+template <> struct ColShape<11> { static constexpr int MA = 3, MB = 3; };
+template <> struct ColShape<12> { static constexpr int MA = 4, MB = 3; };
+template <> struct ColShape<13> { static constexpr int MA = 4, MB = 4; };
+
+template <int RN> struct ColGeo {
+    static constexpr int MA = ColShape<RN>::MA, MB = ColShape<RN>::MB;
+    static constexpr uint32_t R = 1u << RN;
+    static constexpr uint32_t RA = 1u << MA, RB = 1u << MB;
+    static constexpr uint32_t SA = R >> MA, SAP = SA + SA / 32;
+    static constexpr uint32_t NB = 32 * RB, NBP = NB + NB / 32;
+    static_assert(MA + MB + 5 == RN, "three steps cover the column");
+};
+
+// Shared words per column line: the padded length, rounded so that
+// consecutive lines start 32 / min(wc, 32) banks apart.
+__host__ __device__ inline uint32_t col2_stride(uint32_t R, uint32_t wc) {
+    const uint32_t wl = wc < 32 ? wc : 32;
+    return ((R + R / 32 + 31) & ~31u) + 32 / wl;
+}
+
+// Residue mod p of digit i (width w, from coefficient `off` on) of the
+// operand at src (ns limbs, cs coefficients, zero past them).
+template <int PI>
+FFG_DEV_INLINE uint32_t digit_res(const uint64_t *__restrict__ src, uint64_t ns, uint64_t cs, uint64_t off, uint32_t w,
+                                  uint64_t i, const PrimeDev &P) {
+    constexpr uint32_t p = kPrimeC[PI];
+    if (i >= cs) return 0;
+    if (w == 32) {
+        const uint64_t q = off + i; // the 32-bit word
+        uint32_t l = (q >> 1) < ns ? __ldg((const uint32_t *)src + q) : 0;
+        l = min(l, l - p);
+        return min(l, l - p);
+    }
+    const uint64_t bit = (off + i) * w, q = bit >> 6;
+    const uint32_t s = (uint32_t)(bit & 63);
+    const uint64_t lo = q < ns ? __ldg(&src[q]) : 0;
+    const uint64_t hi = s + w > 64 && q + 1 < ns ? __ldg(&src[q + 1]) : 0;
+    const uint64_t v = (s ? (lo >> s) | (hi << (64 - s)) : lo) & ((1ull << w) - 1);
+    uint32_t l = (uint32_t)v;
+    l = min(l, l - p);
+    l = min(l, l - p);
+    return ad<PI>(l, sh<PI>((uint32_t)(v >> 32), make_uint2(P.c32, P.c32s)));
+}
+
+template <int PI, int RN>
+FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FSJob &J, uint32_t *smem) {
+    using Q = ColGeo<RN>;
+    const uint32_t op = G.square ? 0 : (blockIdx.z & 1);
+    const uint32_t C = 1u << G.c, wc = G.wc, wlg = G.wc_lg, LS = col2_stride(Q::R, wc);
+    const uint32_t c0 = blockIdx.x * wc;
+    const uint64_t *src = op ? J.b : J.a;
+    const uint64_t ns = op ? J.nb : J.na, cs = op ? J.cb : J.ca, off = op ? J.off_b : J.off_a;
+    const uint32_t w = J.width;
+
+    if (Q::MA) {
+        const uint2 *tw = P.stw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
+        const uint32_t slots = wc * Q::SA;
+#pragma unroll 1
+        for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
+            const uint32_t c = p & (wc - 1), j = p >> wlg;
+            uint32_t x[Q::RA];
+#pragma unroll
+            for (uint32_t t = 0; t < Q::RA; t++)
+                x[t] = digit_res<PI>(src, ns, cs, off, w, (uint64_t)(j + Q::SA * t) * C + c0 + c, P);
+            dft_dif<PI, Q::MA>(x);
+#pragma unroll
+            for (uint32_t t = 1; t < Q::RA; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * Q::SA + j]));
+            uint32_t *d = smem + c * LS + j + (j >> 5);
+#pragma unroll
+            for (uint32_t t = 0; t < Q::RA; t++) d[t * Q::SAP] = x[t];
+        }
+        __syncthreads();
+    }
+    {
+        const uint2 *tw = P.stw + c_lines.tw_off[5 * 6 + Q::MB];
+        const uint32_t slots = wc * (Q::R / Q::RB);
+#pragma unroll 1
+        for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
+            const uint32_t c = p & (wc - 1), q = p >> wlg, b = q >> 5, j = q & 31;
+            uint32_t *d = smem + c * LS + b * Q::NBP + j;
+            uint32_t x[Q::RB];
+            if (Q::MA) {
+#pragma unroll
+                for (uint32_t t = 0; t < Q::RB; t++) x[t] = d[33 * t];
+            } else {
+#pragma unroll
+                for (uint32_t t = 0; t < Q::RB; t++)
+                    x[t] = digit_res<PI>(src, ns, cs, off, w, (uint64_t)(b * Q::NB + j + 32 * t) * C + c0 + c, P);
+            }
+            dft_dif<PI, Q::MB>(x);
+#pragma unroll
+            for (uint32_t t = 1; t < Q::RB; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * 32 + j]));
+#pragma unroll
+            for (uint32_t t = 0; t < Q::RB; t++) d[33 * t] = x[t];
+        }
+    }
+    __syncthreads();
+    // step C, then ω_L^(n2 k1): position 32 b + t holds frequency
+    // k1 = brev_RN(32 b + t) = brev_5(t) 2^(RN - 5) + brev_(RN - 5)(b)
+    uint32_t *y = (op ? J.yb : J.ya) + (size_t)PI * G.L;
+    const uint32_t slots = wc * (Q::R / 32);
+#pragma unroll 1
+    for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
+        const uint32_t c = p & (wc - 1), b = p >> wlg, n2 = c0 + c;
+        const uint32_t *d = smem + c * LS + 33 * b;
+        uint32_t x[32];
+#pragma unroll
+        for (int t = 0; t < 32; t++) x[t] = d[t];
+        dft_dif<PI, 5>(x);
+        const uint32_t bb = RN > 5 ? __brev(b) >> (32 - (RN - 5)) : 0;
+        uint32_t cur = twm<PI>(P, (uint64_t)n2 * bb % G.L * G.mstep);
+        const uint32_t step = twm<PI>(P, ((uint64_t)n2 << (RN - 5)) % G.L * G.mstep);
+        uint32_t *o = y + (size_t)(32 * b) * C + n2;
+#pragma unroll
+        for (int u = 0; u < 32; u++) {
+            const int t = brev5(u); // compile-time after unrolling
+            o[(size_t)t * C] = mo<PI>(x[t], cur);
+            cur = mo<PI>(cur, step);
+        }
+    }
+}
+
+template <int RN>
+__global__ void __launch_bounds__(kLineThreads, 3) k_col_fwd2(Primes3 P3, FourStep G, FSJobs jobs) {
+    extern __shared__ uint32_t smem[];
+    __shared__ FSJob J;
+    if (threadIdx.x == 0) {
+        const uint32_t i = G.square ? blockIdx.z : (blockIdx.z >> 1);
+        J = jobs.ext ? jobs.ext[i] : jobs.j[i < FFG_FS_JOBS ? i : 0];
+    }
+    __syncthreads();
+    switch (blockIdx.y) {
+    case 0: col_fwd2_body<0, RN>(P3.pr[0], G, J, smem); break;
+    case 1: col_fwd2_body<1, RN>(P3.pr[1], G, J, smem); break;
+    default: col_fwd2_body<2, RN>(P3.pr[2], G, J, smem); break;
+    }
+}
+
+// The final store of the inverse: scaled, written or added into the split's
+// residues.
+template <int PI>
+FFG_DEV_INLINE void col_out(const FourStep &G, const FSJob &J, uint32_t n1, uint32_t n2, uint32_t x, uint2 sc) {
+    const size_t at = (size_t)n1 * (1u << G.c) + n2;
+    const uint32_t v = sh<PI>(x, sc);
+    if (J.yacc) {
+        uint32_t *acc = J.yacc + (size_t)PI * J.acc_stride + J.acc_off + at;
+        *acc = ad<PI>(*acc, v);
+    } else {
+        J.ya[(size_t)PI * G.L + at] = v;
+    }
+}
+
+template <int PI, int RN>
+FFG_DEV_INLINE void col_inv2_body(const PrimeDev &P, const FourStep &G, const FSJob &J, uint32_t *smem) {
+    using Q = ColGeo<RN>;
+    const uint32_t C = 1u << G.c, wc = G.wc, wlg = G.wc_lg, LS = col2_stride(Q::R, wc);
+    const uint32_t c0 = blockIdx.x * wc;
+    const uint32_t *y = J.ya + (size_t)PI * G.L;
+    const uint2 sc = make_uint2(G.scl[PI], G.scls[PI]);
+    {
+        const uint32_t slots = wc * (Q::R / 32);
+#pragma unroll 1
+        for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
+            const uint32_t c = p & (wc - 1), b = p >> wlg;
+            const uint32_t *g = y + (size_t)(32 * b) * C + c0 + c;
+            uint32_t x[32];
+#pragma unroll
+            for (int t = 0; t < 32; t++) x[t] = g[(size_t)t * C];
+            dft_dit<PI, 5>(x);
+            uint32_t *d = smem + c * LS + 33 * b;
+#pragma unroll
+            for (int t = 0; t < 32; t++) d[t] = x[t];
+        }
+    }
+    __syncthreads();
+    {
+        const uint2 *tw = P.istw + c_lines.tw_off[5 * 6 + Q::MB];
+        const uint32_t slots = wc * (Q::R / Q::RB);
+#pragma unroll 1
+        for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
+            const uint32_t c = p & (wc - 1), q = p >> wlg, b = q >> 5, j = q & 31;
+            uint32_t *d = smem + c * LS + b * Q::NBP + j;
+            uint32_t x[Q::RB];
+#pragma unroll
+            for (uint32_t t = 0; t < Q::RB; t++) x[t] = d[33 * t];
+#pragma unroll
+            for (uint32_t t = 1; t < Q::RB; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * 32 + j]));
+            dft_dit<PI, Q::MB>(x);
+            if (Q::MA) {
+#pragma unroll
+                for (uint32_t t = 0; t < Q::RB; t++) d[33 * t] = x[t];
+            } else {
+#pragma unroll
+                for (uint32_t t = 0; t < Q::RB; t++) col_out<PI>(G, J, b * Q::NB + j + 32 * t, c0 + c, x[t], sc);
+            }
+        }
+    }
+    if (!Q::MA) return;
+    __syncthreads();
+    const uint2 *tw = P.istw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
+    const uint32_t slots = wc * Q::SA;
+#pragma unroll 1
+    for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
+        const uint32_t c = p & (wc - 1), j = p >> wlg;
+        const uint32_t *d = smem + c * LS + j + (j >> 5);
+        uint32_t x[Q::RA];
+#pragma unroll
+        for (uint32_t t = 0; t < Q::RA; t++) x[t] = d[t * Q::SAP];
+#pragma unroll
+        for (uint32_t t = 1; t < Q::RA; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * Q::SA + j]));
+        dft_dit<PI, Q::MA>(x);
+#pragma unroll
+        for (uint32_t t = 0; t < Q::RA; t++) col_out<PI>(G, J, j + Q::SA * t, c0 + c, x[t], sc);
+    }
+}
+
+template <int RN>
+__global__ void __launch_bounds__(kLineThreads, 3) k_col_inv2(Primes3 P3, FourStep G, FSJobs jobs) {
+    extern __shared__ uint32_t smem[];
+    __shared__ FSJob J;
+    if (threadIdx.x == 0) J = jobs.ext ? jobs.ext[blockIdx.z] : jobs.j[blockIdx.z < FFG_FS_JOBS ? blockIdx.z : 0];
+    __syncthreads();
+    switch (blockIdx.y) {
+    case 0: col_inv2_body<0, RN>(P3.pr[0], G, J, smem); break;
+    case 1: col_inv2_body<1, RN>(P3.pr[1], G, J, smem); break;
+    default: col_inv2_body<2, RN>(P3.pr[2], G, J, smem); break;
+    }
+}
+
+cudaError_t set_line_consts_cols(const LineConsts &h) { return cudaMemcpyToSymbol(c_lines, &h, sizeof h); }
+
+static size_t col2_smem(const FourStep &G) { return (size_t)G.wc * col2_stride(G.R, G.wc) * sizeof(uint32_t); }
+
+// Whether the fixed-shape column passes take this geometry: power-of-two
+// columns of 2^6 .. 2^13 words, tiles of 8..64 columns that fit in 100 KB.
+bool col2_ok(const FourStep &G) {
+    return !G.r3 && G.rn >= 6 && G.rn <= 13 && G.wc >= 8 && G.wc <= 64 && G.wc == (1u << G.wc_lg) &&
+           G.wc <= (1u << G.c) && col2_smem(G) <= 100 * 1024;
+}
+
+template <int RN>
+static cudaError_t launch_col2_t(bool fwd, const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t nz,
+                                 cudaStream_t st) {
+    const void *k = fwd ? (const void *)k_col_fwd2<RN> : (const void *)k_col_inv2<RN>;
+    static bool attr[2] = {false, false};
+    if (!attr[fwd]) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+        if (e) return e;
+        attr[fwd] = true;
+    }
+    const dim3 grid((1u << G.c) / G.wc, 3, nz);
+    if (fwd) k_col_fwd2<RN><<<grid, kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
+    else k_col_inv2<RN><<<grid, kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
+    return cudaGetLastError();
+}
+
+// nz: grid depth (jobs x operands for the forward pass, jobs for the inverse).
+cudaError_t launch_col2(bool fwd, const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t nz,
+                        cudaStream_t st) {
+    switch (G.rn) {
+    case 6: return launch_col2_t<6>(fwd, P3, G, jobs, nz, st);
+    case 7: return launch_col2_t<7>(fwd, P3, G, jobs, nz, st);
+    case 8: return launch_col2_t<8>(fwd, P3, G, jobs, nz, st);
+    case 9: return launch_col2_t<9>(fwd, P3, G, jobs, nz, st);
+    case 10: return launch_col2_t<10>(fwd, P3, G, jobs, nz, st);
+    case 11: return launch_col2_t<11>(fwd, P3, G, jobs, nz, st);
+    case 12: return launch_col2_t<12>(fwd, P3, G, jobs, nz, st);
+    default: return launch_col2_t<13>(fwd, P3, G, jobs, nz, st);
+    }
+}
+
+} // namespace ffg

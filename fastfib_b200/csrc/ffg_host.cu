@@ -193,20 +193,18 @@ static int fail(int code, const char *fmt, ...) {
                                            __FILE__, __LINE__);                                      \
     } while (0)
 
-// The (stride 2^sl, radix 2^M) pairs the line schedules use, with sl > 0
-// (steps at stride 1 need no twiddles), and their table offsets.
+// Every (stride 2^sl, radix 2^M) step a transform of up to 2^FFG_LINE_LG
+// words can take, with sl > 0 (steps at stride 1 need no twiddles): the line
+// schedules and the fixed-shape row and column kernels pick among them.
+// Returns the table's length; off[sl * 6 + M] is each step's offset.
 static size_t step_table_layout(uint32_t *off) {
     for (int k = 0; k < 15 * 6; k++) off[k] = ~0u;
     size_t total = 0;
-    for (uint32_t n = 1; n <= (uint32_t)FFG_LINE_LG; n++) {
-        int m[4], sl[4];
-        const int k = schedule(n, m, sl);
-        for (int i = 0; i < k; i++) {
-            if (!sl[i] || off[sl[i] * 6 + m[i]] != ~0u) continue;
-            off[sl[i] * 6 + m[i]] = (uint32_t)total;
-            total += (((size_t)1 << m[i]) - 1) << sl[i];
+    for (int sl = 1; sl < FFG_LINE_LG; sl++)
+        for (int M = 1; M <= 5 && sl + M <= FFG_LINE_LG; M++) {
+            off[sl * 6 + M] = (uint32_t)total;
+            total += (((size_t)1 << M) - 1) << sl;
         }
-    }
     return total;
 }
 
@@ -308,6 +306,8 @@ static int build_tables() {
     }
     CK(cudaMemcpy(g.tables, host.data(), per * 3, cudaMemcpyHostToDevice));
     CK(set_line_consts(lc));
+    CK(set_line_consts_rows(lc));
+    CK(set_line_consts_cols(lc));
     return FFG_OK;
 }
 

@@ -223,6 +223,16 @@ cudaError_t launch_school_batch(const SchoolJob *d_jobs, uint32_t count, uint32_
 uint32_t lin_ctas(uint64_t len);                    // CTAs of one linear pass
 
 cudaError_t set_line_consts(const LineConsts &h); // once, before any transform
+cudaError_t set_line_consts_rows(const LineConsts &h); // the same for ffg_rows.cu
+cudaError_t set_line_consts_cols(const LineConsts &h); // and ffg_cols.cu
+// The fixed-shape column passes (ffg_cols.cu) for the geometries col2_ok
+// accepts; nz is the grid depth (jobs x operands forward, jobs inverse).
+bool col2_ok(const FourStep &G);
+cudaError_t launch_col2(bool fwd, const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t nz,
+                        cudaStream_t st);
+// The fixed-shape row pass (ffg_rows.cu) for the geometries row2_ok accepts.
+bool row2_ok(const FourStep &G);
+cudaError_t launch_row2(const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t njobs, cudaStream_t st);
 // Load (and configure) the kernels of one product -- the transforms and the
 // plain CRT -- during set-up, so a later first launch loads no module code.
 cudaError_t ntt_kernels_load();

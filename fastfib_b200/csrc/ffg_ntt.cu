@@ -18,6 +18,8 @@
 // The reference's top radix-16 passes over column chunks and in-cache
 // sub-blocks (src/ntt_conv.c:158-226) play the same roles on the CPU; here
 // each pass is one HBM round trip of the residues.
+#include <cstdlib>
+
 #include "ffg_internal.h"
 #include "ffg_lines.cuh"
 
@@ -269,6 +271,19 @@ cudaError_t launch_conv_small(const Primes3 &P3, const ConvJobs &jobs, uint32_t 
     return cudaGetLastError();
 }
 
+// The fixed-shape row pass (ffg_rows.cu) where it applies; FFG_ROW2=0 keeps
+// the generic one (for comparisons).
+static const bool g_row2 = [] {
+    const char *v = getenv("FFG_ROW2");
+    return !(v && v[0] == '0');
+}();
+// The fixed-shape column passes (ffg_cols.cu) likewise; FFG_COL2=0 keeps the
+// generic ones.
+static const bool g_col2 = [] {
+    const char *v = getenv("FFG_COL2");
+    return !(v && v[0] == '0');
+}();
+
 // Geometry the four-step kernels support: lines of at least 2 words (a
 // stride-1 step has at least radix 2), rows of at least 4 words and column
 // tiles of 4..64 words within a row (16-byte row loads), tiles that fit
@@ -290,18 +305,34 @@ cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs 
     // algorithmic bytes: one 4-byte read and write of every residue per pass
     // (twiddles excluded); the first pass reads limbs instead of residues
     const double res = 3.0 * 4.0 * (double)G.L * njobs;
+    const bool col2 = g_col2 && col2_ok(G);
     prof_begin(PK_COL_FWD, st);
-    k_col_fwd<<<dim3(tiles, 3, njobs * nops), 256, sm_col, st>>>(P3, G, jobs);
+    if (col2) {
+        e = launch_col2(true, P3, G, jobs, njobs * nops, st);
+    } else {
+        k_col_fwd<<<dim3(tiles, 3, njobs * nops), 256, sm_col, st>>>(P3, G, jobs);
+        e = cudaGetLastError();
+    }
     prof_end(PK_COL_FWD, st, res * nops + limb_bytes);
-    if ((e = cudaGetLastError())) return e;
+    if (e) return e;
     prof_begin(PK_ROW_CONV, st);
-    k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, jobs);
+    if (g_row2 && row2_ok(G)) {
+        e = launch_row2(P3, G, jobs, njobs, st);
+    } else {
+        k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, jobs);
+        e = cudaGetLastError();
+    }
     prof_end(PK_ROW_CONV, st, res * (nops + 1));
-    if ((e = cudaGetLastError())) return e;
+    if (e) return e;
     prof_begin(PK_COL_INV, st);
-    k_col_inv<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, jobs);
+    if (col2) {
+        e = launch_col2(false, P3, G, jobs, njobs, st);
+    } else {
+        k_col_inv<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, jobs);
+        e = cudaGetLastError();
+    }
     prof_end(PK_COL_INV, st, res * 2);
-    return cudaGetLastError();
+    return e;
 }
 
 // The split multiply's passes, each over a list of jobs sharing geometry G.
@@ -323,9 +354,14 @@ cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJobs &jo
     const uint32_t tiles = (1u << G.c) / G.wc;
     const double res = 3.0 * 4.0 * (double)G.L * njobs;
     prof_begin(PK_COL_FWD, st);
-    k_col_fwd<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, jobs);
+    if (g_col2 && col2_ok(G)) {
+        e = launch_col2(true, P3, G, jobs, njobs, st);
+    } else {
+        k_col_fwd<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, jobs);
+        e = cudaGetLastError();
+    }
     prof_end(PK_COL_FWD, st, res + limb_bytes);
-    if ((e = cudaGetLastError())) return e;
+    if (e) return e;
     prof_begin(PK_ROW_CONV, st);
     k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, jobs);
     prof_end(PK_ROW_CONV, st, res * 2);
@@ -349,9 +385,14 @@ cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob &job, 
     prof_end(PK_ROW_CONV, st, res * (2.0 * pairs + 1.0));
     if ((e = cudaGetLastError())) return e;
     prof_begin(PK_COL_INV, st);
-    k_col_inv<<<dim3(tiles, 3, 1), 256, sm_col, st>>>(P3, G, one);
+    if (g_col2 && col2_ok(G)) {
+        e = launch_col2(false, P3, G, one, 1, st);
+    } else {
+        k_col_inv<<<dim3(tiles, 3, 1), 256, sm_col, st>>>(P3, G, one);
+        e = cudaGetLastError();
+    }
     prof_end(PK_COL_INV, st, res * 3.0);
-    return cudaGetLastError();
+    return e;
 }
 
 } // namespace ffg
