@@ -253,6 +253,78 @@ def ntt_microbench(limbs, square, steps, warmup):
                            "of": peak_src}}
 
 
+def ntt_suite(steps=3, warmup=3, sizes=(1 << 14, 1 << 17, 1 << 20, 1 << 22), cpu=True):
+    """The multiply microbench: random operands (seeded, uniform 64-bit limbs)
+    of 2^14, 2^17, 2^20 and 2^22 limbs, squares and distinct products, each at
+    the reference's own plan ("ntt") and with the transform length forced to
+    2^k ("ntt_pow2") and to 3 2^k ("ntt_r3").  Device ms per product (CUDA
+    events on the stream, L2 flushed before each, operands resident), every
+    product checked modulo four 64-bit primes, and beside the plan's figure
+    the reference's own big_mul / big_sqr on this host's cores (oracle/_ref,
+    fastest of 3 calls, all pool threads)."""
+    import numpy as np
+    import torch
+    import fastfib_b200 as ff
+    torch.cuda.set_device(0)
+    ff.set_device(0)
+    ff.init(4 * max(sizes))  # tables up to 2^25: the forced 3 2^k lengths fit, no split
+    ref = None
+    if cpu:
+        from oracle import Reference, reference_available
+        ref = Reference() if reference_available() else None
+    with open(GOLD_FP) as f:
+        primes = [int(p) for p in json.load(f)["primes"]]
+    rng = np.random.default_rng(88172645463325252 % 2**63)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    # a stream of our own: the library runs on the stream it is given, and the
+    # events must be recorded on that same stream
+    ts_stream = torch.cuda.Stream()
+    stream = ts_stream.cuda_stream
+    rows = []
+    for n in sizes:
+        a = rng.integers(0, 2**64, n, dtype=np.uint64)
+        b = rng.integers(0, 2**64, n, dtype=np.uint64)
+        a[-1] |= np.uint64(1 << 63)
+        b[-1] |= np.uint64(1 << 63)
+        da = torch.from_numpy(a.view(np.int64)).cuda()
+        db = torch.from_numpy(b.view(np.int64)).cuda()
+        out = torch.zeros(2 * n + 1, dtype=torch.int64, device="cuda")
+        xa, xb = int.from_bytes(a.tobytes(), "little"), int.from_bytes(b.tobytes(), "little")
+        for sq in (True, False):
+            want = [(xa % p) * ((xa if sq else xb) % p) % p for p in primes]
+            row = {"limbs": n, "square": sq}
+            for m in ("ntt", "ntt_pow2", "ntt_r3"):
+                job = [{"a": da.data_ptr(), "b": (da if sq else db).data_ptr(), "na": n, "nb": n, "bits_a": 64 * n,
+                        "bits_b": 64 * n, "out": out.data_ptr(), "square": sq, "method": m}]
+                for _ in range(warmup):
+                    ff.mul_batch_device(job, stream)
+                ts = []
+                for i in range(steps):
+                    flush.fill_(i & 0xFF)
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(ts_stream)
+                    ff.mul_batch_device(job, stream)
+                    e1.record(ts_stream)
+                    torch.cuda.synchronize()
+                    ts.append(e0.elapsed_time(e1))
+                z = int.from_bytes(out.cpu().numpy().tobytes(), "little")
+                ok = all(z % p == w for p, w in zip(primes, want))
+                pl = ff.plan(64 * n, 64 * n, sq) if m == "ntt" else None
+                row[m] = {"ms": statistics.mean(ts), "bit_exact": ok}
+                if pl:
+                    row["plan"] = {"width": pl["width"], "L": pl["L"], "split": pl["split"]}
+            if ref is not None:
+                row["cpu_reference_ms"] = ref.time_mul(a, None if sq else b, square=sq, reps=3) * 1e3
+                row["speedup_vs_cpu"] = row["cpu_reference_ms"] / row["ntt"]["ms"]
+            rows.append(row)
+        del da, db, out
+    return {"rows": rows, "cpu": {"kind": "reference" if ref else None, "cores": ref.cpus() if ref else None,
+                                  "sample": "big_mul / big_sqr on the same operands, fastest of 3 calls, "
+                                            "NTT tables built first"},
+            "bit_exact": all(r[m]["bit_exact"] for r in rows for m in ("ntt", "ntt_pow2", "ntt_r3"))}
+
+
 def job_ms(totals, steps, world, device="cuda"):
     """Replicas: each of `world` ranks ran `steps` chains in totals = [device
     ms, host ms]; the job's time is the max over ranks (an all-reduce MAX when
@@ -326,21 +398,25 @@ def run_uneven(count=4096, reps=3, seed=4):
         offs.append(oo)
         oa, ob, oo = oa + a.size, ob + b.size, oo + a.size + b.size + 1
 
+    # a stream of our own, given to the library and timed with events
+    # recorded on it (the library runs each call on the stream it is given)
+    ts_stream = torch.cuda.Stream()
+
     def timed(fn):
         ts = []
         for r in range(reps + 1):
             flush.fill_(r & 0xFF)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
+            e0.record(ts_stream)
             fn()
-            e1.record()
+            e1.record(ts_stream)
             torch.cuda.synchronize()
             if r:
                 ts.append(e0.elapsed_time(e1))
         return statistics.mean(ts)
 
-    stream = torch.cuda.current_stream().cuda_stream
+    stream = ts_stream.cuda_stream
     res = {}
     for m in ("plain", "learned"):
         js = [dict(j, method=m) for j in jobs]
@@ -368,11 +444,42 @@ def run_uneven(count=4096, reps=3, seed=4):
     ff.mul_batch(pairs, "learned")
     e2e = (time.perf_counter() - t) * 1e3
     in_bytes = 8 * (int(flat_a.numel()) + int(flat_b.numel()))
+    # the floor of that host call: the same bytes over PCIe each way, pinned
+    # host buffers, one copy each (timed with events on a stream of our own)
+    hin = torch.empty(in_bytes, dtype=torch.uint8, pin_memory=True)
+    hout = torch.empty(8 * out_len, dtype=torch.uint8, pin_memory=True)
+    dbuf = torch.empty(max(in_bytes, 8 * out_len), dtype=torch.uint8, device=dev)
+    with torch.cuda.stream(ts_stream):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(ts_stream)
+        dbuf[:in_bytes].copy_(hin, non_blocking=True)
+        e1.record(ts_stream)
+        hout.copy_(dbuf[:8 * out_len], non_blocking=True)
+        e2.record(ts_stream)
+    torch.cuda.synchronize()
+    pcie = {"h2d_ms": e0.elapsed_time(e1), "d2h_ms": e1.elapsed_time(e2)}
+    del hin, hout, dbuf
+    # device-only times: the batch's launches captured once and replayed
+    # (host planning outside the clock)
+    graph_ms = {m: ff.time_batch([dict(j, method=m) for j in jobs], reps=3) for m in ("plain", "learned")}
+    cpu = None
+    from oracle import Reference, reference_available
+    if reference_available():
+        ref = Reference()
+        cpu = {"value": ref.time_mul_batch(pairs) * 1e3, "unit": "ms", "cores": ref.cpus(), "kind": "reference",
+               "sample": f"the same {count} products by the reference's big_mul, one after another (each on "
+                         f"all pool threads), NTT tables built first; one run"}
     return {"workload": f"{count} products, operands log-uniform 2^10..2^24 bits, aspect <= 16, seed {seed}",
+            "cpu_baseline": cpu,
             "plain_unbatched_ms": res["plain_unbatched"], "plain_ms": res["plain"], "learned_ms": res["learned"],
             "learned_vs_plain": res["plain"] / res["learned"],
             "batched_learned_vs_plain_unbatched": res["plain_unbatched"] / res["learned"],
-            "e2e_ms": e2e, "h2d_bytes": in_bytes, "d2h_bytes": 8 * out_len, "bit_exact": ok,
+            "e2e_ms": e2e, "h2d_bytes": in_bytes, "d2h_bytes": 8 * out_len, "pcie_copies_ms": pcie,
+            "graph_replay_device_ms": graph_ms,
+            "timing": "plain / learned / unbatched: CUDA events on the call's stream around the whole call "
+                      "(host planning included); graph_replay_device_ms: the launches alone; e2e_ms: the "
+                      "host API with operands and products in host memory",
+            "bit_exact": ok,
             "l2": "flushed before every timed run"}
 
 
@@ -385,7 +492,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-f1e9", action="store_true", help="skip the extra F(10^9) measurement")
-    ap.add_argument("--config", default="fib", choices=["fib", "ntt", "uneven"],
+    ap.add_argument("--config", default="fib", choices=["fib", "ntt", "ntt-suite", "uneven"],
                     help="fib: F(n) (the headline); ntt: one NTT product of --limbs limbs; "
                          "uneven: the uneven product stream, plain against learned dispatch")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-stream figures in the fib line")
@@ -403,6 +510,12 @@ def main():
         return run_reference(args, rank, world)
     if args.config == "ntt":
         return run_ntt_microbench(args)
+    if args.config == "ntt-suite":
+        r = ntt_suite(steps=args.steps, warmup=args.warmup, cpu=not args.no_cpu_baseline)
+        print(json.dumps({"metric": "NTT multiply ms (microbench: 2^14..2^22 limbs, squares and products, "
+                                    "plan / forced 2^k / forced 3 2^k)", "unit": "ms", "higher_is_better": False,
+                          "steps": args.steps, "warmup": args.warmup, "dtype": "u32", "config": r}), flush=True)
+        return 0 if r["bit_exact"] else 1
     if args.config == "uneven":
         r = run_uneven(reps=args.steps)
         print(json.dumps({"metric": "uneven product stream ms (4096 products), learned vs plain dispatch",
@@ -545,6 +658,8 @@ def main():
             line["ntt_l2e24"] = {"workload": nb["config"]["workload"], "L": nb["config"]["plan"]["L"],
                                  "ms": nb["value"], "passes": nb["ntt_passes"], "families": nb["families"],
                                  "bit_exact": nb["bit_exact"]}
+        if not args.no_ntt and world == 1:
+            line["ntt_suite"] = ntt_suite(cpu=not args.no_cpu_baseline)
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.n)
         print(json.dumps(line), flush=True)

@@ -324,22 +324,27 @@ def mul_batch(pairs, method="ntt") -> list:
     (a, b) with b None for a square; method names one of METHODS, or is a list
     with one name per product."""
     arrs, jobs = [], (Job * max(1, len(pairs)))()
-    outs = []
+    # one output area for the whole batch (written only where the products
+    # land); each result is a view of its part
+    sizes = [(_arr(a).size, (_arr(a) if b is None else _arr(b)).size) for a, b in pairs]
+    area = np.empty(sum(x + y for x, y in sizes), dtype=np.uint64)
+    base = area.ctypes.data
+    offs, o = [], 0
     for i, (a, b) in enumerate(pairs):
         a = _arr(a)
         sq = b is None
         b = a if sq else _arr(b)
-        out = np.zeros(a.size + b.size, dtype=np.uint64)
         arrs += [a, b]
-        outs.append(out)
+        offs.append(o)
         m = method[i] if isinstance(method, (list, tuple)) else method
         j = jobs[i]
         j.a, j.b = a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p)
         j.na, j.nb = a.size, b.size
-        j.out = out.ctypes.data_as(_u64p)
+        j.out = ctypes.cast(base + 8 * o, _u64p)
         j.square, j.method = int(sq), METHODS[m]
+        o += a.size + b.size
     _check(lib().ffg_mul_batch_host(jobs, len(pairs)))
-    return [outs[i][: jobs[i].nout].copy() for i in range(len(pairs))]
+    return [area[offs[i]: offs[i] + jobs[i].nout] for i in range(len(pairs))]
 
 
 def mul_batch_device(jobs, stream: int = 0) -> None:

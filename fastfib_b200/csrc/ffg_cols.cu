@@ -80,7 +80,7 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
     using Q = ColGeo<RN>;
     const uint32_t op = G.square ? 0 : (blockIdx.z & 1);
     const uint32_t C = 1u << G.c, wc = G.wc, wlg = G.wc_lg, LS = col2_stride(Q::R, wc);
-    const uint32_t c0 = blockIdx.x * wc;
+    const uint32_t c0 = blockIdx.y * wc; // blockIdx.x is the prime: a tile's three CTAs share its limbs in L2
     const uint64_t *src = op ? J.b : J.a;
     const uint64_t ns = op ? J.nb : J.na, cs = op ? J.cb : J.ca, off = op ? J.off_b : J.off_a;
     const uint32_t w = J.width;
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kLineThreads, 3) k_col_fwd2(Primes3 P3, FourSt
         J = jobs.ext ? jobs.ext[i] : jobs.j[i < FFG_FS_JOBS ? i : 0];
     }
     __syncthreads();
-    switch (blockIdx.y) {
+    switch (blockIdx.x) {
     case 0: col_fwd2_body<0, RN>(P3.pr[0], G, J, smem); break;
     case 1: col_fwd2_body<1, RN>(P3.pr[1], G, J, smem); break;
     default: col_fwd2_body<2, RN>(P3.pr[2], G, J, smem); break;
@@ -281,9 +281,9 @@ static cudaError_t launch_col2_t(bool fwd, const Primes3 &P3, const FourStep &G,
         if (e) return e;
         attr[fwd] = true;
     }
-    const dim3 grid((1u << G.c) / G.wc, 3, nz);
-    if (fwd) k_col_fwd2<RN><<<grid, kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
-    else k_col_inv2<RN><<<grid, kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
+    const uint32_t tiles = (1u << G.c) / G.wc;
+    if (fwd) k_col_fwd2<RN><<<dim3(3, tiles, nz), kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
+    else k_col_inv2<RN><<<dim3(tiles, 3, nz), kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
     return cudaGetLastError();
 }
 

@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <map>
 #include <tuple>
@@ -1857,6 +1858,38 @@ extern "C" int ffg_time_batch(ffg_job *jobs, size_t count, int reps, double *ms)
     return FFG_OK;
 }
 
+// Host-side copies of a batch, split over threads: jobs [j0, j1) in `parts`
+// ranges of about equal bytes, fn(i) per job.
+template <typename F>
+static void par_jobs(size_t j0, size_t j1, const std::vector<uint64_t> &bytes_upto, F fn) {
+    const size_t n = j1 - j0;
+    const uint64_t total = bytes_upto[j1] - bytes_upto[j0];
+    unsigned hw = std::thread::hardware_concurrency();
+    unsigned parts = (unsigned)std::min<uint64_t>(std::min<size_t>(n, hw ? hw : 4), 1 + total / (1u << 20));
+    if (parts > 16) parts = 16;
+    if (parts <= 1) {
+        for (size_t i = j0; i < j1; i++) fn(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    size_t lo = j0;
+    for (unsigned k = 1; k <= parts && lo < j1; k++) {
+        const uint64_t goal = bytes_upto[j0] + total * k / parts;
+        size_t hi = lo + 1;
+        while (hi < j1 && bytes_upto[hi] < goal) hi++;
+        if (k == parts) hi = j1;
+        th.emplace_back([lo, hi, &fn] {
+            for (size_t i = lo; i < hi; i++) fn(i);
+        });
+        lo = hi;
+    }
+    for (auto &t : th) t.join();
+}
+
+// ffg_mul_batch_host: the operands are staged into pinned memory by several
+// threads, a slice of jobs at a time, each slice's host-to-device copy
+// overlapping the staging of the next; the products come back the same way,
+// a slice's device-to-host copy overlapping the unstaging of the one before.
 extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
     std::lock_guard<std::recursive_mutex> lk(g_mu);
     int rc = ensure_ready();
@@ -1866,7 +1899,8 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
     CK(cudaStreamSynchronize(st));
     arena_reset();
     // normalized sizes, one staging image of every operand, one result area
-    std::vector<uint64_t> na(count), nb(count), ba(count), bb(count), aoff(count), boff(count), roff(count);
+    std::vector<uint64_t> na(count), nb(count), ba(count), bb(count), aoff(count + 1), boff(count), roff(count + 1);
+    std::vector<uint64_t> in_upto(count + 1), out_upto(count + 1);
     uint64_t in_limbs = 0, out_limbs = 0;
     for (size_t i = 0; i < count; i++) {
         ffg_job &u = jobs[i];
@@ -1875,12 +1909,16 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
         na[i] = std::max<uint64_t>(1, (ba[i] + 63) / 64);
         nb[i] = std::max<uint64_t>(1, (bb[i] + 63) / 64);
         aoff[i] = in_limbs;
+        in_upto[i] = in_limbs * 8;
         in_limbs += na[i];
         boff[i] = u.square ? aoff[i] : in_limbs;
         if (!u.square) in_limbs += nb[i];
         roff[i] = out_limbs;
+        out_upto[i] = out_limbs * 8;
         out_limbs += na[i] + nb[i] + 1;
     }
+    aoff[count] = in_limbs, roff[count] = out_limbs;
+    in_upto[count] = in_limbs * 8, out_upto[count] = out_limbs * 8;
     uint64_t *din = (uint64_t *)arena_alloc(std::max<uint64_t>(1, in_limbs) * 8);
     uint64_t *dout = (uint64_t *)arena_alloc(std::max<uint64_t>(1, out_limbs) * 8);
     if (!din || !dout) return fail(FFG_E_NOMEM, "device arena: batch operands");
@@ -1896,16 +1934,32 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
         }
     } in_buf{nullptr, st}, out_buf{nullptr, st};
     uint64_t *hin = (uint64_t *)(in_buf.p = pinned_get(std::max<uint64_t>(1, in_limbs) * 8));
-    if (!hin) return fail(FFG_E_NOMEM, "pinned staging");
-    for (size_t i = 0; i < count; i++) {
-        memcpy(hin + aoff[i], jobs[i].a, std::min(na[i], jobs[i].na) * 8);
-        if (na[i] > jobs[i].na) hin[aoff[i]] = 0;
-        if (!jobs[i].square) {
-            memcpy(hin + boff[i], jobs[i].b, std::min(nb[i], jobs[i].nb) * 8);
-            if (nb[i] > jobs[i].nb) hin[boff[i]] = 0;
+    uint64_t *hout = (uint64_t *)(out_buf.p = pinned_get(std::max<uint64_t>(1, out_limbs) * 8));
+    if (!hin || !hout) return fail(FFG_E_NOMEM, "pinned staging");
+    // slices of about 1/8 of the bytes each (whole jobs)
+    auto slices = [&](const std::vector<uint64_t> &upto) {
+        std::vector<size_t> cut{0};
+        for (int k = 1; k < 8; k++) {
+            size_t i = cut.back();
+            while (i < count && upto[i] < upto[count] * k / 8) i++;
+            if (i > cut.back()) cut.push_back(i);
         }
+        if (cut.back() != count) cut.push_back(count);
+        return cut;
+    };
+    const std::vector<size_t> icut = slices(in_upto);
+    for (size_t k = 0; k + 1 < icut.size(); k++) {
+        const size_t j0 = icut[k], j1 = icut[k + 1];
+        par_jobs(j0, j1, in_upto, [&](size_t i) {
+            memcpy(hin + aoff[i], jobs[i].a, std::min(na[i], jobs[i].na) * 8);
+            if (na[i] > jobs[i].na) hin[aoff[i]] = 0;
+            if (!jobs[i].square) {
+                memcpy(hin + boff[i], jobs[i].b, std::min(nb[i], jobs[i].nb) * 8);
+                if (nb[i] > jobs[i].nb) hin[boff[i]] = 0;
+            }
+        });
+        CK(cudaMemcpyAsync(din + aoff[j0], hin + aoff[j0], (aoff[j1] - aoff[j0]) * 8, cudaMemcpyHostToDevice, st));
     }
-    CK(cudaMemcpyAsync(din, hin, in_limbs * 8, cudaMemcpyHostToDevice, st));
     std::vector<int> sqv(count), meth(count);
     for (size_t i = 0; i < count; i++) sqv[i] = jobs[i].square != 0, meth[i] = jobs[i].method;
     if ((rc = learned_resolve(ba.data(), bb.data(), sqv.data(), meth.data(), count, st))) return rc;
@@ -1920,15 +1974,29 @@ extern "C" int ffg_mul_batch_host(ffg_job *jobs, size_t count) {
         bj.push_back(J);
     }
     if ((rc = run_batch(bj, st))) return rc;
-    uint64_t *hout = (uint64_t *)(out_buf.p = pinned_get(std::max<uint64_t>(1, out_limbs) * 8));
-    if (!hout) return fail(FFG_E_NOMEM, "pinned staging");
-    CK(cudaMemcpyAsync(hout, dout, out_limbs * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (size_t i = 0; i < count; i++) {
-        uint64_t n = na[i] + nb[i];
-        while (n > 1 && hout[roff[i] + n - 1] == 0) n--;
-        memcpy(jobs[i].out, hout + roff[i], n * 8);
-        jobs[i].nout = n;
+    const std::vector<size_t> ocut = slices(out_upto);
+    std::vector<cudaEvent_t> ev(ocut.size());
+    for (auto &e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    struct Events {
+        std::vector<cudaEvent_t> &v;
+        ~Events() {
+            for (auto e : v)
+                if (e) cudaEventDestroy(e);
+        }
+    } ev_guard{ev};
+    for (size_t k = 0; k + 1 < ocut.size(); k++) {
+        const size_t j0 = ocut[k], j1 = ocut[k + 1];
+        CK(cudaMemcpyAsync(hout + roff[j0], dout + roff[j0], (roff[j1] - roff[j0]) * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(ev[k], st));
+    }
+    for (size_t k = 0; k + 1 < ocut.size(); k++) {
+        CK(cudaEventSynchronize(ev[k]));
+        par_jobs(ocut[k], ocut[k + 1], out_upto, [&](size_t i) {
+            uint64_t n = na[i] + nb[i];
+            while (n > 1 && hout[roff[i] + n - 1] == 0) n--;
+            memcpy(jobs[i].out, hout + roff[i], n * 8);
+            jobs[i].nout = n;
+        });
     }
     return FFG_OK;
 }

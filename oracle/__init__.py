@@ -219,6 +219,32 @@ class Reference(_Lib):
     def cpus(self) -> int:
         return self.lib.ffref_cpus()
 
+    def time_mul(self, a, b=None, square=False, reps=3) -> float:
+        """Seconds of the fastest of `reps` big_mul / big_sqr calls, timed in C."""
+        a, pa, na = _arr(a)
+        if square or b is None:
+            pb, nb = pa, na
+        else:
+            b, pb, nb = _arr(b)
+        f = self.lib.ffref_time_mul
+        f.restype = ctypes.c_double
+        f.argtypes = [_u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int]
+        return f(pa, na, pb, nb, int(bool(square or b is None)), reps)
+
+    def time_mul_batch(self, pairs) -> float:
+        """Seconds for big_mul over every (a, b) pair, one after another, timed in C."""
+        na = np.array([a.size for a, _ in pairs], dtype=np.uint64)
+        nb = np.array([b.size for _, b in pairs], dtype=np.uint64)
+        aoff = np.concatenate([[0], np.cumsum(na)[:-1]]).astype(np.uint64)
+        boff = np.concatenate([[0], np.cumsum(nb)[:-1]]).astype(np.uint64)
+        A = np.ascontiguousarray(np.concatenate([a for a, _ in pairs]), dtype=np.uint64)
+        B = np.ascontiguousarray(np.concatenate([b for _, b in pairs]), dtype=np.uint64)
+        f = self.lib.ffref_time_mul_batch
+        f.restype = ctypes.c_double
+        f.argtypes = [_u64p, _szp, _szp, _u64p, _szp, _szp, ctypes.c_size_t]
+        sp = lambda x: x.ctypes.data_as(_szp)  # noqa: E731
+        return f(A.ctypes.data_as(_u64p), sp(aoff), sp(na), B.ctypes.data_as(_u64p), sp(boff), sp(nb), len(pairs))
+
 
 def reference_available() -> bool:
     return os.path.exists(REF_SO)

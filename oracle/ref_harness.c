@@ -74,3 +74,42 @@ double ffref_seconds(void) { return plat_seconds(); }
 
 /** Logical CPUs the reference's pool uses (src/pool.c, plat_cpu_count). */
 int ffref_cpus(void) { return plat_cpu_count(); }
+
+/** The CPU baseline of the multiply microbench: `reps` calls of the
+    reference's big_mul / big_sqr (its own threshold dispatch, NTT and thread
+    pool, its NTT tables built first) on one operand pair, the results freed
+    unread; returns the seconds of the fastest call, timed with the
+    reference's clock. */
+double ffref_time_mul(const uint64_t *a, size_t na, const uint64_t *b, size_t nb, int square, int reps) {
+    Big A = ffref_view(a, na), B = ffref_view(b, nb);
+    ntt_init(na + nb); /* tables first (untimed), as fibonacci() does */
+    double best = 1e30;
+    for (int i = 0; i < reps; i++) {
+        double t = plat_seconds();
+        Big r = square ? big_sqr(&A) : big_mul(&A, &B);
+        t = plat_seconds() - t;
+        big_free(&r);
+        if (t < best) best = t;
+    }
+    return best;
+}
+
+/** The CPU baseline of a batch of independent products: products i < count
+    of operands a + aoff[i] (na[i] limbs) and b + boff[i] (nb[i] limbs), one
+    big_mul after another as the reference computes independent products
+    (src/decimal.c:177-203 runs its products one at a time, each spread over
+    the pool); returns the seconds for the whole batch. */
+double ffref_time_mul_batch(const uint64_t *a, const size_t *aoff, const size_t *na, const uint64_t *b,
+                            const size_t *boff, const size_t *nb, size_t count) {
+    size_t most = 0;
+    for (size_t i = 0; i < count; i++)
+        if (na[i] + nb[i] > most) most = na[i] + nb[i];
+    ntt_init(most); /* tables first (untimed) */
+    double t = plat_seconds();
+    for (size_t i = 0; i < count; i++) {
+        Big A = ffref_view(a + aoff[i], na[i]), B = ffref_view(b + boff[i], nb[i]);
+        Big r = big_mul(&A, &B);
+        big_free(&r);
+    }
+    return plat_seconds() - t;
+}

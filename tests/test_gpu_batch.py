@@ -121,3 +121,44 @@ def test_large_group_one_cta(ff, L, square):
     assert plan["L"] == L and plan["kernel"] == 1, plan
     got = ff.mul_batch(pairs)
     assert [limbs_to_int(g) for g in got] == exact(pairs)
+
+
+@pytest.mark.parametrize("n", [1 << 20, 1 << 22])
+def test_microbench_sizes_every_length_family(ff, n):
+    """The multiply microbench's large cases: distinct products and squares of
+    random 2^20- and 2^22-limb operands at the reference's plan and with the
+    transform length forced to 2^k and to 3 2^k (L up to 3 2^23).  The three
+    results must agree limb for limb, and match the exact product modulo three
+    64-bit primes and modulo 2^128 (the low limbs), with the exact bit length."""
+    torch = pytest.importorskip("torch")
+    ff.init(1 << 24)  # transform tables up to 2^25: no product here takes the split
+    assert ff.plan(64 * n, 64 * n, False)["split"] == 0
+    rng = np.random.default_rng(n + 11)
+    a = rng.integers(0, 2**64, n, dtype=np.uint64)
+    b = rng.integers(0, 2**64, n, dtype=np.uint64)
+    a[-1] |= np.uint64(1 << 63)
+    b[-1] |= np.uint64(1 << 62)
+    xa, xb = limbs_to_int(a), limbs_to_int(b)
+    da = torch.from_numpy(a.view(np.int64)).cuda()
+    db = torch.from_numpy(b.view(np.int64)).cuda()
+    for sq in (False, True):
+        y = xa if sq else xb
+        outs = []
+        for m in ("ntt", "ntt_pow2", "ntt_r3"):
+            out = torch.full((2 * n + 1,), -1, dtype=torch.int64, device="cuda")
+            ff.mul_batch_device([{"a": da.data_ptr(), "b": (da if sq else db).data_ptr(), "na": n, "nb": n,
+                                  "bits_a": 64 * n, "bits_b": 64 * n, "out": out.data_ptr(), "square": sq,
+                                  "method": m}])
+            torch.cuda.synchronize()
+            outs.append(out.cpu().numpy().view(np.uint64).copy())
+        assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+        z = limbs_to_int(outs[0])
+        for p in PRIMES:
+            assert z % p == (xa % p) * (y % p) % p
+        assert z % 2**128 == (xa % 2**128) * (y % 2**128) % 2**128
+        # bit length: the top two limbs of the operands fix it to within one
+        # bit; the exact value follows from the product of the top parts
+        top = (limbs_to_int(a[-2:]) * limbs_to_int((a if sq else b)[-2:])).bit_length()
+        lo_bits = 64 * (n - 2) * 2
+        assert z.bit_length() in (top + lo_bits, top + lo_bits + 1)
+    del da, db
