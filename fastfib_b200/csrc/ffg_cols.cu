@@ -1,12 +1,15 @@
 // The four-step column passes with the column length fixed at compile time,
-// for columns of R = 2^RN words (6 <= RN <= 13).
+// for columns of R = 2^RN or 3 2^RN words (6 <= RN <= 13).
 //
 // A CTA holds a tile of wc columns x R rows in shared memory, one padded
-// line per column.  The length-R transform of each column is three radix
-// steps (decimation in frequency forward, in time inverse):
-//   A: radix 2^MA at stride R / 2^MA (absent when RN <= 9),
+// line per column.  The length-2^RN transform of each column (of each of its
+// three blocks of 2^RN words when R = 3 2^RN) is three radix steps
+// (decimation in frequency forward, in time inverse):
+//   A: radix 2^MA at stride 2^RN / 2^MA (absent when RN <= 9),
 //   B: radix 2^MB at stride 32,
-//   C: radix 32 at stride 1 (no step twiddles).
+//   C: radix 32 at stride 1 (no step twiddles);
+// with R = 3 2^RN a radix-3 step at stride 2^RN comes first (forward) or
+// last (inverse), as in the generic line transforms (r3_dif / r3_dit).
 // k_col_fwd2: the first step reads the operand's digits straight from its
 //   limbs (the reference's Src reader, src/ntt_kernels.c:29-74, one digit per
 //   word), step C ends with the four-step twiddle ω_L^(n2 k1) and stores the
@@ -75,30 +78,50 @@ FFG_DEV_INLINE uint32_t digit_res(const uint64_t *__restrict__ src, uint64_t ns,
     return ad<PI>(l, sh<PI>((uint32_t)(v >> 32), make_uint2(P.c32, P.c32s)));
 }
 
-template <int PI, int RN>
+
+// The digit of row r, column n2 of the operand's four-step layout.
+#define FFG_COL_DIGIT(r) digit_res<PI>(src, ns, cs, off, w, (uint64_t)(r) * C + c0 + c, P)
+
+template <int PI, int RN, bool R3>
 FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FSJob &J, uint32_t *smem) {
     using Q = ColGeo<RN>;
+    constexpr uint32_t NBLK = R3 ? 3 : 1, BP = Q::R + Q::R / 32; // blocks and padded block length
     const uint32_t op = G.square ? 0 : (blockIdx.z & 1);
-    const uint32_t C = 1u << G.c, wc = G.wc, wlg = G.wc_lg, LS = col2_stride(Q::R, wc);
-    const uint32_t c0 = blockIdx.y * wc; // blockIdx.x is the prime: a tile's three CTAs share its limbs in L2
+    const uint32_t C = 1u << G.c, wc = G.wc, wlg = G.wc_lg, LS = col2_stride(NBLK * Q::R, wc);
+    const uint32_t c0 = blockIdx.x * wc;
     const uint64_t *src = op ? J.b : J.a;
     const uint64_t ns = op ? J.nb : J.na, cs = op ? J.cb : J.ca, off = op ? J.off_b : J.off_a;
     const uint32_t w = J.width;
 
+    if (R3) { // radix 3 at stride 2^RN, straight from the digits
+        constexpr uint32_t p = kPrimeC[PI];
+        const uint32_t slots = wc * Q::R;
+#pragma unroll 1
+        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+            const uint32_t c = s & (wc - 1), j = s >> wlg;
+            const uint32_t x0 = FFG_COL_DIGIT(j), x1 = FFG_COL_DIGIT(j + Q::R), x2 = FFG_COL_DIGIT(j + 2 * Q::R);
+            const uint4 t = __ldg(&P.r3f[Q::R + j]);
+            const uint32_t u = sh<PI>(x1 - x2 + p, c_lines.w3[PI]);
+            uint32_t *d = smem + c * LS + j + (j >> 5);
+            d[0] = ad<PI>(ad<PI>(x0, x1), x2);
+            d[BP] = sh<PI>(ad<PI>(sb<PI>(x0, x2), u), make_uint2(t.x, t.y));
+            d[2 * BP] = sh<PI>(sb<PI>(sb<PI>(x0, x1), u), make_uint2(t.z, t.w));
+        }
+        __syncthreads();
+    }
     if (Q::MA) {
         const uint2 *tw = P.stw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
-        const uint32_t slots = wc * Q::SA;
+        const uint32_t slots = wc * NBLK * Q::SA;
 #pragma unroll 1
-        for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
-            const uint32_t c = p & (wc - 1), j = p >> wlg;
+        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+            const uint32_t c = s & (wc - 1), g = s >> wlg, q = g >> (RN - Q::MA), j = g & (Q::SA - 1);
+            uint32_t *d = smem + c * LS + q * BP + j + (j >> 5);
             uint32_t x[Q::RA];
 #pragma unroll
-            for (uint32_t t = 0; t < Q::RA; t++)
-                x[t] = digit_res<PI>(src, ns, cs, off, w, (uint64_t)(j + Q::SA * t) * C + c0 + c, P);
+            for (uint32_t t = 0; t < Q::RA; t++) x[t] = R3 ? d[t * Q::SAP] : FFG_COL_DIGIT(j + Q::SA * t);
             dft_dif<PI, Q::MA>(x);
 #pragma unroll
             for (uint32_t t = 1; t < Q::RA; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * Q::SA + j]));
-            uint32_t *d = smem + c * LS + j + (j >> 5);
 #pragma unroll
             for (uint32_t t = 0; t < Q::RA; t++) d[t * Q::SAP] = x[t];
         }
@@ -106,20 +129,16 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
     }
     {
         const uint2 *tw = P.stw + c_lines.tw_off[5 * 6 + Q::MB];
-        const uint32_t slots = wc * (Q::R / Q::RB);
+        const uint32_t slots = wc * NBLK * (Q::R / Q::RB);
 #pragma unroll 1
-        for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
-            const uint32_t c = p & (wc - 1), q = p >> wlg, b = q >> 5, j = q & 31;
+        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+            // blocks of NB words run on through the radix-3 blocks (NB divides 2^RN)
+            const uint32_t c = s & (wc - 1), g = s >> wlg, b = g >> 5, j = g & 31;
             uint32_t *d = smem + c * LS + b * Q::NBP + j;
             uint32_t x[Q::RB];
-            if (Q::MA) {
 #pragma unroll
-                for (uint32_t t = 0; t < Q::RB; t++) x[t] = d[33 * t];
-            } else {
-#pragma unroll
-                for (uint32_t t = 0; t < Q::RB; t++)
-                    x[t] = digit_res<PI>(src, ns, cs, off, w, (uint64_t)(b * Q::NB + j + 32 * t) * C + c0 + c, P);
-            }
+            for (uint32_t t = 0; t < Q::RB; t++)
+                x[t] = (Q::MA || R3) ? d[33 * t] : FFG_COL_DIGIT(b * Q::NB + j + 32 * t);
             dft_dif<PI, Q::MB>(x);
 #pragma unroll
             for (uint32_t t = 1; t < Q::RB; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * 32 + j]));
@@ -128,21 +147,24 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
         }
     }
     __syncthreads();
-    // step C, then ω_L^(n2 k1): position 32 b + t holds frequency
-    // k1 = brev_RN(32 b + t) = brev_5(t) 2^(RN - 5) + brev_(RN - 5)(b)
+    // step C, then ω_L^(n2 k1): position q 2^RN + 32 b + t holds frequency
+    // k1 = q + m brev_RN(32 b + t) = q + m (brev_5(t) 2^(RN - 5) + brev_(RN - 5)(b)),
+    // m = 3 with the radix-3 step (q its block), else m = 1 and q = 0
+    constexpr uint32_t m3 = R3 ? 3 : 1;
     uint32_t *y = (op ? J.yb : J.ya) + (size_t)PI * G.L;
-    const uint32_t slots = wc * (Q::R / 32);
+    const uint32_t slots = wc * NBLK * (Q::R / 32);
 #pragma unroll 1
-    for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
-        const uint32_t c = p & (wc - 1), b = p >> wlg, n2 = c0 + c;
-        const uint32_t *d = smem + c * LS + 33 * b;
+    for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+        const uint32_t c = s & (wc - 1), b = s >> wlg, n2 = c0 + c;
+        const uint32_t q = b >> (RN - 5), bl = b & ((Q::R >> 5) - 1);
+        const uint32_t *d = smem + c * LS + q * BP + 33 * bl;
         uint32_t x[32];
 #pragma unroll
         for (int t = 0; t < 32; t++) x[t] = d[t];
         dft_dif<PI, 5>(x);
-        const uint32_t bb = RN > 5 ? __brev(b) >> (32 - (RN - 5)) : 0;
-        uint32_t cur = twm<PI>(P, (uint64_t)n2 * bb % G.L * G.mstep);
-        const uint32_t step = twm<PI>(P, ((uint64_t)n2 << (RN - 5)) % G.L * G.mstep);
+        const uint32_t bb = __brev(bl) >> (32 - (RN - 5));
+        uint32_t cur = twm<PI>(P, (uint64_t)n2 * (q + m3 * bb) % G.L * G.mstep);
+        const uint32_t step = twm<PI>(P, ((uint64_t)n2 * m3 << (RN - 5)) % G.L * G.mstep);
         uint32_t *o = y + (size_t)(32 * b) * C + n2;
 #pragma unroll
         for (int u = 0; u < 32; u++) {
@@ -152,9 +174,10 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
         }
     }
 }
+#undef FFG_COL_DIGIT
 
-template <int RN>
-__global__ void __launch_bounds__(kLineThreads, 3) k_col_fwd2(Primes3 P3, FourStep G, FSJobs jobs) {
+template <int RN, bool R3>
+__global__ void __launch_bounds__(kLineThreads, R3 ? 2 : 3) k_col_fwd2(Primes3 P3, FourStep G, FSJobs jobs) {
     extern __shared__ uint32_t smem[];
     __shared__ FSJob J;
     if (threadIdx.x == 0) {
@@ -162,10 +185,10 @@ __global__ void __launch_bounds__(kLineThreads, 3) k_col_fwd2(Primes3 P3, FourSt
         J = jobs.ext ? jobs.ext[i] : jobs.j[i < FFG_FS_JOBS ? i : 0];
     }
     __syncthreads();
-    switch (blockIdx.x) {
-    case 0: col_fwd2_body<0, RN>(P3.pr[0], G, J, smem); break;
-    case 1: col_fwd2_body<1, RN>(P3.pr[1], G, J, smem); break;
-    default: col_fwd2_body<2, RN>(P3.pr[2], G, J, smem); break;
+    switch (blockIdx.y) {
+    case 0: col_fwd2_body<0, RN, R3>(P3.pr[0], G, J, smem); break;
+    case 1: col_fwd2_body<1, RN, R3>(P3.pr[1], G, J, smem); break;
+    default: col_fwd2_body<2, RN, R3>(P3.pr[2], G, J, smem); break;
     }
 }
 
@@ -183,24 +206,26 @@ FFG_DEV_INLINE void col_out(const FourStep &G, const FSJob &J, uint32_t n1, uint
     }
 }
 
-template <int PI, int RN>
+template <int PI, int RN, bool R3>
 FFG_DEV_INLINE void col_inv2_body(const PrimeDev &P, const FourStep &G, const FSJob &J, uint32_t *smem) {
     using Q = ColGeo<RN>;
-    const uint32_t C = 1u << G.c, wc = G.wc, wlg = G.wc_lg, LS = col2_stride(Q::R, wc);
+    constexpr uint32_t NBLK = R3 ? 3 : 1, BP = Q::R + Q::R / 32;
+    const uint32_t C = 1u << G.c, wc = G.wc, wlg = G.wc_lg, LS = col2_stride(NBLK * Q::R, wc);
     const uint32_t c0 = blockIdx.x * wc;
     const uint32_t *y = J.ya + (size_t)PI * G.L;
     const uint2 sc = make_uint2(G.scl[PI], G.scls[PI]);
     {
-        const uint32_t slots = wc * (Q::R / 32);
+        const uint32_t slots = wc * NBLK * (Q::R / 32);
 #pragma unroll 1
-        for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
-            const uint32_t c = p & (wc - 1), b = p >> wlg;
+        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+            const uint32_t c = s & (wc - 1), b = s >> wlg;
+            const uint32_t q = b >> (RN - 5), bl = b & ((Q::R >> 5) - 1);
             const uint32_t *g = y + (size_t)(32 * b) * C + c0 + c;
             uint32_t x[32];
 #pragma unroll
             for (int t = 0; t < 32; t++) x[t] = g[(size_t)t * C];
             dft_dit<PI, 5>(x);
-            uint32_t *d = smem + c * LS + 33 * b;
+            uint32_t *d = smem + c * LS + q * BP + 33 * bl;
 #pragma unroll
             for (int t = 0; t < 32; t++) d[t] = x[t];
         }
@@ -208,10 +233,10 @@ FFG_DEV_INLINE void col_inv2_body(const PrimeDev &P, const FourStep &G, const FS
     __syncthreads();
     {
         const uint2 *tw = P.istw + c_lines.tw_off[5 * 6 + Q::MB];
-        const uint32_t slots = wc * (Q::R / Q::RB);
+        const uint32_t slots = wc * NBLK * (Q::R / Q::RB);
 #pragma unroll 1
-        for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
-            const uint32_t c = p & (wc - 1), q = p >> wlg, b = q >> 5, j = q & 31;
+        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+            const uint32_t c = s & (wc - 1), g = s >> wlg, b = g >> 5, j = g & 31;
             uint32_t *d = smem + c * LS + b * Q::NBP + j;
             uint32_t x[Q::RB];
 #pragma unroll
@@ -219,7 +244,7 @@ FFG_DEV_INLINE void col_inv2_body(const PrimeDev &P, const FourStep &G, const FS
 #pragma unroll
             for (uint32_t t = 1; t < Q::RB; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * 32 + j]));
             dft_dit<PI, Q::MB>(x);
-            if (Q::MA) {
+            if (Q::MA || R3) {
 #pragma unroll
                 for (uint32_t t = 0; t < Q::RB; t++) d[33 * t] = x[t];
             } else {
@@ -228,35 +253,60 @@ FFG_DEV_INLINE void col_inv2_body(const PrimeDev &P, const FourStep &G, const FS
             }
         }
     }
-    if (!Q::MA) return;
+    if (!Q::MA && !R3) return;
     __syncthreads();
-    const uint2 *tw = P.istw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
-    const uint32_t slots = wc * Q::SA;
+    if (Q::MA) {
+        const uint2 *tw = P.istw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
+        const uint32_t slots = wc * NBLK * Q::SA;
 #pragma unroll 1
-    for (uint32_t p = threadIdx.x; p < slots; p += kLineThreads) {
-        const uint32_t c = p & (wc - 1), j = p >> wlg;
+        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+            const uint32_t c = s & (wc - 1), g = s >> wlg, q = g >> (RN - Q::MA), j = g & (Q::SA - 1);
+            uint32_t *d = smem + c * LS + q * BP + j + (j >> 5);
+            uint32_t x[Q::RA];
+#pragma unroll
+            for (uint32_t t = 0; t < Q::RA; t++) x[t] = d[t * Q::SAP];
+#pragma unroll
+            for (uint32_t t = 1; t < Q::RA; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * Q::SA + j]));
+            dft_dit<PI, Q::MA>(x);
+            if (R3) {
+#pragma unroll
+                for (uint32_t t = 0; t < Q::RA; t++) d[t * Q::SAP] = x[t];
+            } else {
+#pragma unroll
+                for (uint32_t t = 0; t < Q::RA; t++) col_out<PI>(G, J, j + Q::SA * t, c0 + c, x[t], sc);
+            }
+        }
+        if (!R3) return;
+        __syncthreads();
+    }
+    // radix 3 at stride 2^RN (the generic r3_dit), scaled and stored
+    constexpr uint32_t p = kPrimeC[PI];
+    const uint32_t slots = wc * Q::R;
+#pragma unroll 1
+    for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+        const uint32_t c = s & (wc - 1), j = s >> wlg;
         const uint32_t *d = smem + c * LS + j + (j >> 5);
-        uint32_t x[Q::RA];
-#pragma unroll
-        for (uint32_t t = 0; t < Q::RA; t++) x[t] = d[t * Q::SAP];
-#pragma unroll
-        for (uint32_t t = 1; t < Q::RA; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * Q::SA + j]));
-        dft_dit<PI, Q::MA>(x);
-#pragma unroll
-        for (uint32_t t = 0; t < Q::RA; t++) col_out<PI>(G, J, j + Q::SA * t, c0 + c, x[t], sc);
+        const uint4 t = __ldg(&P.r3i[Q::R + j]);
+        const uint32_t y0 = d[0];
+        const uint32_t z1 = sh<PI>(d[BP], make_uint2(t.x, t.y));
+        const uint32_t z2 = sh<PI>(d[2 * BP], make_uint2(t.z, t.w));
+        const uint32_t u = sh<PI>(z1 - z2 + p, c_lines.v3[PI]);
+        col_out<PI>(G, J, j, c0 + c, ad<PI>(ad<PI>(y0, z1), z2), sc);
+        col_out<PI>(G, J, j + Q::R, c0 + c, ad<PI>(sb<PI>(y0, z2), u), sc);
+        col_out<PI>(G, J, j + 2 * Q::R, c0 + c, sb<PI>(sb<PI>(y0, z1), u), sc);
     }
 }
 
-template <int RN>
-__global__ void __launch_bounds__(kLineThreads, 3) k_col_inv2(Primes3 P3, FourStep G, FSJobs jobs) {
+template <int RN, bool R3>
+__global__ void __launch_bounds__(kLineThreads, R3 ? 2 : 3) k_col_inv2(Primes3 P3, FourStep G, FSJobs jobs) {
     extern __shared__ uint32_t smem[];
     __shared__ FSJob J;
     if (threadIdx.x == 0) J = jobs.ext ? jobs.ext[blockIdx.z] : jobs.j[blockIdx.z < FFG_FS_JOBS ? blockIdx.z : 0];
     __syncthreads();
     switch (blockIdx.y) {
-    case 0: col_inv2_body<0, RN>(P3.pr[0], G, J, smem); break;
-    case 1: col_inv2_body<1, RN>(P3.pr[1], G, J, smem); break;
-    default: col_inv2_body<2, RN>(P3.pr[2], G, J, smem); break;
+    case 0: col_inv2_body<0, RN, R3>(P3.pr[0], G, J, smem); break;
+    case 1: col_inv2_body<1, RN, R3>(P3.pr[1], G, J, smem); break;
+    default: col_inv2_body<2, RN, R3>(P3.pr[2], G, J, smem); break;
     }
 }
 
@@ -264,42 +314,50 @@ cudaError_t set_line_consts_cols(const LineConsts &h) { return cudaMemcpyToSymbo
 
 static size_t col2_smem(const FourStep &G) { return (size_t)G.wc * col2_stride(G.R, G.wc) * sizeof(uint32_t); }
 
-// Whether the fixed-shape column passes take this geometry: power-of-two
-// columns of 2^6 .. 2^13 words, tiles of 8..64 columns that fit in 100 KB.
+// Whether the fixed-shape column passes take this geometry: columns of
+// 2^6 .. 2^13 words (3 2^6 .. 3 2^12 with the radix-3 step, as far as its
+// twiddle tables go), tiles of 8..64
+// columns that fit in 110 KB of shared memory.
 bool col2_ok(const FourStep &G) {
-    return !G.r3 && G.rn >= 6 && G.rn <= 13 && G.wc >= 8 && G.wc <= 64 && G.wc == (1u << G.wc_lg) &&
-           G.wc <= (1u << G.c) && col2_smem(G) <= 100 * 1024;
+    return G.rn >= 6 && G.rn <= (G.r3 ? 12u : 13u) && G.wc >= 8 && G.wc <= 64 && G.wc == (1u << G.wc_lg) && G.wc <= (1u << G.c) &&
+           col2_smem(G) <= 110 * 1024;
 }
 
-template <int RN>
+template <int RN, bool R3>
 static cudaError_t launch_col2_t(bool fwd, const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t nz,
                                  cudaStream_t st) {
-    const void *k = fwd ? (const void *)k_col_fwd2<RN> : (const void *)k_col_inv2<RN>;
+    const void *k = fwd ? (const void *)k_col_fwd2<RN, R3> : (const void *)k_col_inv2<RN, R3>;
     static bool attr[2] = {false, false};
     if (!attr[fwd]) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024);
         if (e) return e;
         attr[fwd] = true;
     }
-    const uint32_t tiles = (1u << G.c) / G.wc;
-    if (fwd) k_col_fwd2<RN><<<dim3(3, tiles, nz), kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
-    else k_col_inv2<RN><<<dim3(tiles, 3, nz), kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
+    const dim3 grid((1u << G.c) / G.wc, 3, nz);
+    if (fwd) k_col_fwd2<RN, R3><<<grid, kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
+    else k_col_inv2<RN, R3><<<grid, kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
     return cudaGetLastError();
+}
+
+template <bool R3>
+static cudaError_t launch_col2_r(bool fwd, const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t nz,
+                                 cudaStream_t st) {
+    switch (G.rn) {
+    case 6: return launch_col2_t<6, R3>(fwd, P3, G, jobs, nz, st);
+    case 7: return launch_col2_t<7, R3>(fwd, P3, G, jobs, nz, st);
+    case 8: return launch_col2_t<8, R3>(fwd, P3, G, jobs, nz, st);
+    case 9: return launch_col2_t<9, R3>(fwd, P3, G, jobs, nz, st);
+    case 10: return launch_col2_t<10, R3>(fwd, P3, G, jobs, nz, st);
+    case 11: return launch_col2_t<11, R3>(fwd, P3, G, jobs, nz, st);
+    case 12: return launch_col2_t<12, R3>(fwd, P3, G, jobs, nz, st);
+    default: return launch_col2_t<13, R3>(fwd, P3, G, jobs, nz, st);
+    }
 }
 
 // nz: grid depth (jobs x operands for the forward pass, jobs for the inverse).
 cudaError_t launch_col2(bool fwd, const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t nz,
                         cudaStream_t st) {
-    switch (G.rn) {
-    case 6: return launch_col2_t<6>(fwd, P3, G, jobs, nz, st);
-    case 7: return launch_col2_t<7>(fwd, P3, G, jobs, nz, st);
-    case 8: return launch_col2_t<8>(fwd, P3, G, jobs, nz, st);
-    case 9: return launch_col2_t<9>(fwd, P3, G, jobs, nz, st);
-    case 10: return launch_col2_t<10>(fwd, P3, G, jobs, nz, st);
-    case 11: return launch_col2_t<11>(fwd, P3, G, jobs, nz, st);
-    case 12: return launch_col2_t<12>(fwd, P3, G, jobs, nz, st);
-    default: return launch_col2_t<13>(fwd, P3, G, jobs, nz, st);
-    }
+    return G.r3 ? launch_col2_r<true>(fwd, P3, G, jobs, nz, st) : launch_col2_r<false>(fwd, P3, G, jobs, nz, st);
 }
 
 } // namespace ffg
