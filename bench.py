@@ -483,6 +483,74 @@ def run_uneven(count=4096, reps=3, seed=4):
             "l2": "flushed before every timed run"}
 
 
+def run_uneven_sharded(world, rank, count=4096, seed=4, reps=3):
+    """The uneven product stream split over the ranks by predicted cost
+    (fastfib_b200/shard.py: longest-processing-time over the library's own
+    plans), each rank's share one batched call on its GPU (operands resident),
+    timed with CUDA events on the call's stream, the max over ranks; then the
+    products gathered on rank 0 over the process group and checked there
+    modulo three 64-bit primes.  Every rank takes the same collective steps."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import fastfib_b200 as ff
+    from fastfib_b200.shard import gather_products, imbalance, partition, product_cost
+    from fastfib_b200.workload import uneven_products
+    ff.init(1 << 22)
+    pairs = uneven_products(seed=seed, count=count)
+    costs = [product_cost(a.size, b.size, False) for a, b in pairs]
+    shares = partition(costs, world)
+    share = shares[rank]
+    dev = torch.device("cuda")
+    mine = [pairs[i] for i in share]
+    fa = torch.from_numpy(np.concatenate([a for a, _ in mine]).view(np.int64)).to(dev)
+    fb = torch.from_numpy(np.concatenate([b for _, b in mine]).view(np.int64)).to(dev)
+    out = torch.empty(sum(a.size + b.size + 1 for a, b in mine), dtype=torch.int64, device=dev)
+    jobs, oa, ob, oo, offs = [], 0, 0, 0, []
+    for a, b in mine:
+        jobs.append({"a": fa.data_ptr() + 8 * oa, "b": fb.data_ptr() + 8 * ob, "na": a.size, "nb": b.size,
+                     "bits_a": 64 * a.size, "bits_b": 64 * b.size, "out": out.data_ptr() + 8 * oo, "method": "plain"})
+        offs.append(oo)
+        oa, ob, oo = oa + a.size, ob + b.size, oo + a.size + b.size + 1
+    ts_stream = torch.cuda.Stream()
+    ff.mul_batch_device(jobs, ts_stream.cuda_stream)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ts_stream)
+        ff.mul_batch_device(jobs, ts_stream.cuda_stream)
+        e1.record(ts_stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    t = torch.tensor([statistics.mean(ts)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    host = out.cpu().numpy().view(np.uint64)
+    local = {i: host[o: o + a.size + b.size + 1] for i, o, (a, b) in zip(share, offs, mine)}
+    dist.barrier()
+    t0 = time.perf_counter()
+    got = gather_products(local, count, dst=0)
+    gather_ms = (time.perf_counter() - t0) * 1e3
+    if rank != 0:
+        return None
+    with open(GOLD_FP) as f:
+        primes = [int(p) for p in json.load(f)["primes"]][:3]
+    ok = all(got[i] is not None for i in range(count))
+    for (a, b), z in zip(pairs, got):
+        if not ok:
+            break
+        x, y = int.from_bytes(a.tobytes(), "little"), int.from_bytes(b.tobytes(), "little")
+        zz = int.from_bytes(z.tobytes(), "little")
+        ok = all(zz % p == (x % p) * (y % p) % p for p in primes)
+    return {"workload": f"{count} products, operands log-uniform 2^10..2^24 bits, aspect <= 16, seed {seed}, "
+                        f"split by product over {world} ranks (plain dispatch)",
+            "ms": float(t.item()), "ranks": world, "products_per_rank": [len(x) for x in shares],
+            "cost_imbalance": imbalance(costs, shares), "gather_ms": gather_ms, "bit_exact": ok,
+            "scaling": "strong (one fixed batch)",
+            "timing": "CUDA events around each rank's batched call on its stream, max over ranks"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -590,6 +658,7 @@ def main():
     ff.profile(False)
 
     value, e2e = job_ms([sum(dev_ms), sum(e2e_ms)], args.steps, world)
+    sharded = run_uneven_sharded(world, rank) if world > 1 and not args.no_uneven else None
 
     extra = {}
     if rank == 0 and args.n == 10**8 and world == 1 and not args.no_f1e9:
@@ -649,6 +718,8 @@ def main():
             "clocks": clk.summary(),
             "f1e9": extra or None,
         }
+        if sharded:
+            line["uneven_sharded"] = sharded
         if not args.no_uneven and world == 1:
             line["uneven"] = run_uneven(reps=3)
         if not args.no_decimal and world == 1 and args.n == 10**8:

@@ -148,7 +148,7 @@ def main(argv=None):
     ap.add_argument("--out", default=ff.TUNING_PATH)
     ap.add_argument("--data", default="", help="also save the timing rows (npz)")
     args = ap.parse_args(argv)
-    ff.init(1 << 22)
+    ff.init(1 << 24)  # tables to 2^25: geometry for every length up to 2^24 (and 3 2^23)
     t0 = time.time()
     geometry = [] if args.no_geometry else tune_geometry(log=print)
     t1 = time.time()

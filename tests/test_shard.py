@@ -1,0 +1,105 @@
+"""CPU tests of the by-product sharding (fastfib_b200/shard.py): the cost
+partition of the uneven product stream over 2..8 ranks, and the sharded
+batch with its gather on two gloo ranks, each rank's share computed by the
+oracle, whose union on rank 0 must be exactly the single-rank result."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _costs(ff, pairs):
+    from fastfib_b200.shard import product_cost
+    ff.lib().ffg_set_ntt_max_L(1 << 25)
+    return [product_cost(a.size, (a if b is None else b).size, b is None) for a, b in pairs]
+
+
+def test_partition_of_the_uneven_stream(ff):
+    from fastfib_b200.shard import imbalance, partition
+    from fastfib_b200.workload import uneven_sizes
+    sizes = uneven_sizes(seed=4, count=4096)
+    pairs = [(np.zeros((x + 63) // 64, np.uint64), np.zeros((y + 63) // 64, np.uint64)) for x, y in sizes]
+    costs = _costs(ff, pairs)
+    for ranks in (2, 3, 4, 8):
+        shares = partition(costs, ranks)
+        flat = sorted(i for s in shares for i in s)
+        assert flat == list(range(len(pairs)))  # every product once
+        assert imbalance(costs, shares) < 0.10, ranks
+
+
+def test_partition_edge_cases():
+    from fastfib_b200.shard import imbalance, partition
+    assert partition([], 3) == [[], [], []]
+    assert partition([5.0], 2) in ([[0], []], [[], [0]])
+    shares = partition([1.0] * 10, 4)
+    assert sorted(len(s) for s in shares) == [2, 2, 3, 3]
+    assert imbalance([1.0] * 8, partition([1.0] * 8, 4)) == 0.0
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _pairs():
+    from fastfib_b200.workload import uneven_products
+    pairs = uneven_products(seed=9, count=120, lo=6, hi=15)
+    return pairs + [(a, None) for a, _ in uneven_products(seed=10, count=30, lo=6, hi=14)]
+
+
+def _rank(rank, world, port, q):
+    import sys
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import fastfib_b200 as ff
+        from fastfib_b200.shard import mul_batch_sharded, partition, product_cost
+        from oracle import Oracle
+        ff.lib().ffg_set_ntt_max_L(1 << 25)
+        o = Oracle()
+        o.ntt_init(1 << 16)
+        pairs = _pairs()
+
+        def mul(ps):  # this rank's share, on the CPU checker
+            return [o.mul(a, b) if b is not None else o.mul(a) for a, b in ps]
+
+        got, share = mul_batch_sharded(pairs, group=None, dst=0, mul=mul)
+        costs = [product_cost(a.size, (a if b is None else b).size, b is None) for a, b in pairs]
+        assert share == partition(costs, world)[rank]
+        res = None
+        if rank == 0:
+            want = mul(pairs)
+            res = all(np.array_equal(g, w) for g, w in zip(got, want)) and len(got) == len(want)
+        else:
+            res = got is None
+        dist.barrier()
+        q.put((rank, res, len(share)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_batch_on_two_gloo_ranks():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    res = {}
+    for _ in range(2):
+        r, ok, n = q.get(timeout=10)
+        res[r] = (ok, n)
+    assert res[0][0] is True and res[1][0] is True
+    assert res[0][1] + res[1][1] == len(_pairs()) and res[0][1] > 0 and res[1][1] > 0
