@@ -17,7 +17,7 @@
 // k_col_inv2: step C^-1 reads the row pass's output straight from global
 //   memory, the last step scales by 2^32 / L and stores (or adds into the
 //   split's residues), as k_col_inv.
-// Each step maps thread slots p = threadIdx.x + 256 k to (column p mod wc,
+// Each step maps thread slots p = threadIdx.x + blockDim.x k to (column p mod wc,
 // group p / wc), so a warp's global accesses cover min(wc, 32) consecutive
 // words of each row it touches, and consecutive lines start 32 / min(wc, 32)
 // banks apart, so no shared access has a bank conflict.
@@ -97,7 +97,7 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
         constexpr uint32_t p = kPrimeC[PI];
         const uint32_t slots = wc * Q::R;
 #pragma unroll 1
-        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
             const uint32_t c = s & (wc - 1), j = s >> wlg;
             const uint32_t x0 = FFG_COL_DIGIT(j), x1 = FFG_COL_DIGIT(j + Q::R), x2 = FFG_COL_DIGIT(j + 2 * Q::R);
             const uint4 t = __ldg(&P.r3f[Q::R + j]);
@@ -113,7 +113,7 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
         const uint2 *tw = P.stw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
         const uint32_t slots = wc * NBLK * Q::SA;
 #pragma unroll 1
-        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
             const uint32_t c = s & (wc - 1), g = s >> wlg, q = g >> (RN - Q::MA), j = g & (Q::SA - 1);
             uint32_t *d = smem + c * LS + q * BP + j + (j >> 5);
             uint32_t x[Q::RA];
@@ -131,7 +131,7 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
         const uint2 *tw = P.stw + c_lines.tw_off[5 * 6 + Q::MB];
         const uint32_t slots = wc * NBLK * (Q::R / Q::RB);
 #pragma unroll 1
-        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
             // blocks of NB words run on through the radix-3 blocks (NB divides 2^RN)
             const uint32_t c = s & (wc - 1), g = s >> wlg, b = g >> 5, j = g & 31;
             uint32_t *d = smem + c * LS + b * Q::NBP + j;
@@ -154,7 +154,7 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
     uint32_t *y = (op ? J.yb : J.ya) + (size_t)PI * G.L;
     const uint32_t slots = wc * NBLK * (Q::R / 32);
 #pragma unroll 1
-    for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+    for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
         const uint32_t c = s & (wc - 1), b = s >> wlg, n2 = c0 + c;
         const uint32_t q = b >> (RN - 5), bl = b & ((Q::R >> 5) - 1);
         const uint32_t *d = smem + c * LS + q * BP + 33 * bl;
@@ -217,7 +217,7 @@ FFG_DEV_INLINE void col_inv2_body(const PrimeDev &P, const FourStep &G, const FS
     {
         const uint32_t slots = wc * NBLK * (Q::R / 32);
 #pragma unroll 1
-        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
             const uint32_t c = s & (wc - 1), b = s >> wlg;
             const uint32_t q = b >> (RN - 5), bl = b & ((Q::R >> 5) - 1);
             const uint32_t *g = y + (size_t)(32 * b) * C + c0 + c;
@@ -235,7 +235,7 @@ FFG_DEV_INLINE void col_inv2_body(const PrimeDev &P, const FourStep &G, const FS
         const uint2 *tw = P.istw + c_lines.tw_off[5 * 6 + Q::MB];
         const uint32_t slots = wc * NBLK * (Q::R / Q::RB);
 #pragma unroll 1
-        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
             const uint32_t c = s & (wc - 1), g = s >> wlg, b = g >> 5, j = g & 31;
             uint32_t *d = smem + c * LS + b * Q::NBP + j;
             uint32_t x[Q::RB];
@@ -259,7 +259,7 @@ FFG_DEV_INLINE void col_inv2_body(const PrimeDev &P, const FourStep &G, const FS
         const uint2 *tw = P.istw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
         const uint32_t slots = wc * NBLK * Q::SA;
 #pragma unroll 1
-        for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
             const uint32_t c = s & (wc - 1), g = s >> wlg, q = g >> (RN - Q::MA), j = g & (Q::SA - 1);
             uint32_t *d = smem + c * LS + q * BP + j + (j >> 5);
             uint32_t x[Q::RA];
@@ -283,7 +283,7 @@ FFG_DEV_INLINE void col_inv2_body(const PrimeDev &P, const FourStep &G, const FS
     constexpr uint32_t p = kPrimeC[PI];
     const uint32_t slots = wc * Q::R;
 #pragma unroll 1
-    for (uint32_t s = threadIdx.x; s < slots; s += kLineThreads) {
+    for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
         const uint32_t c = s & (wc - 1), j = s >> wlg;
         const uint32_t *d = smem + c * LS + j + (j >> 5);
         const uint4 t = __ldg(&P.r3i[Q::R + j]);
@@ -334,8 +334,13 @@ static cudaError_t launch_col2_t(bool fwd, const Primes3 &P3, const FourStep &G,
         attr[fwd] = true;
     }
     const dim3 grid((1u << G.c) / G.wc, 3, nz);
-    if (fwd) k_col_fwd2<RN, R3><<<grid, kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
-    else k_col_inv2<RN, R3><<<grid, kLineThreads, col2_smem(G), st>>>(P3, G, jobs);
+    // threads per CTA: about one per four groups of the radix-32 step (short
+    // columns give a tile few groups; idle threads would only wait)
+    const uint32_t groups = G.wc * (uint32_t)(G.R / 32);
+    uint32_t threads = groups * 4 < kLineThreads ? groups * 4 : kLineThreads;
+    threads = threads < 64 ? 64 : (threads + 31) & ~31u;
+    if (fwd) k_col_fwd2<RN, R3><<<grid, threads, col2_smem(G), st>>>(P3, G, jobs);
+    else k_col_inv2<RN, R3><<<grid, threads, col2_smem(G), st>>>(P3, G, jobs);
     return cudaGetLastError();
 }
 

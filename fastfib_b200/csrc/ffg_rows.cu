@@ -1,7 +1,8 @@
 // The four-step row pass with its shape fixed at compile time, for rows of
 // C = 2^CLG words (9 <= CLG <= 13).
 //
-// A row is C / 32 threads; a CTA of 256 threads holds 256 / (C / 32) rows.
+// A row is C / 32 threads; a CTA holds up to 256 / (C / 32) rows, fewer when
+// that would leave SMs idle (the launch picks the rows per CTA).
 // The forward transform of a row is three radix steps of decimation in
 // frequency (the last two may merge into one when CLG <= 10):
 //   A: radix 2^MA at stride SA = C / 2^MA, straight from global memory;
@@ -38,7 +39,7 @@ template <int CLG> struct RowGeo {
     static constexpr int MA = RowShape<CLG>::MA, MB = RowShape<CLG>::MB;
     static constexpr uint32_t C = 1u << CLG;
     static constexpr uint32_t T = C / 32;          // threads per row
-    static constexpr uint32_t ROWS = 256 / T;      // rows per CTA
+    static constexpr uint32_t ROWS = 256 / T;      // most rows per CTA
     static constexpr uint32_t RA = 1u << MA, RB = 1u << MB;
     static constexpr uint32_t SA = C >> MA;        // stride of step A
     static constexpr uint32_t SAP = SA + SA / 32;  // its padded distance
@@ -130,7 +131,7 @@ template <int PI, int CLG, bool SQ>
 FFG_DEV_INLINE void row2_body(const PrimeDev &P, const FourStep &G, const FSJob &J, uint32_t *smem) {
     using Q = RowGeo<CLG>;
     const uint32_t r = threadIdx.x / Q::T, tau = threadIdx.x % Q::T;
-    const uint32_t pos = blockIdx.x * Q::ROWS + r;
+    const uint32_t pos = blockIdx.x * (blockDim.x / Q::T) + r;
     const size_t rowoff = (size_t)PI * G.L + (size_t)pos * Q::C;
     uint32_t *ya = J.ya + rowoff;
     const uint32_t *yb = SQ ? ya : J.yb + rowoff;
@@ -253,14 +254,20 @@ template <int CLG, bool SQ>
 static cudaError_t launch_row2_t(const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t njobs,
                                  cudaStream_t st) {
     using Q = RowGeo<CLG>;
-    const size_t sm = (size_t)Q::ROWS * (SQ ? 1 : 2) * Q::LS * sizeof(uint32_t);
+    const size_t smax = (size_t)Q::ROWS * (SQ ? 1 : 2) * Q::LS * sizeof(uint32_t);
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_row2<CLG, SQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = cudaFuncSetAttribute(k_row2<CLG, SQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
         if (e) return e;
         attr = true;
     }
-    k_row2<CLG, SQ><<<dim3(G.R / Q::ROWS, 3, njobs), 256, sm, st>>>(P3, G, jobs);
+    // rows per CTA: as many as fit 256 threads, halved while the launch would
+    // have fewer than three CTAs per SM (short rows of a mid-size product)
+    uint32_t rows = Q::ROWS;
+    while (rows > 1 && (uint64_t)(G.R / rows) * 3 * njobs < 3 * 148) rows >>= 1;
+    while (rows > 1 && G.R % rows) rows >>= 1;
+    const size_t sm = (size_t)rows * (SQ ? 1 : 2) * Q::LS * sizeof(uint32_t);
+    k_row2<CLG, SQ><<<dim3(G.R / rows, 3, njobs), rows * Q::T, sm, st>>>(P3, G, jobs);
     return cudaGetLastError();
 }
 
@@ -269,12 +276,8 @@ static cudaError_t launch_row2_t(const Primes3 &P3, const FourStep &G, const FSJ
 cudaError_t set_line_consts_rows(const LineConsts &h) { return cudaMemcpyToSymbol(c_lines, &h, sizeof h); }
 
 // Whether the fixed-shape row pass takes this geometry (ROW_CONV rows of
-// 2^9 .. 2^13 words, the row count a multiple of the rows per CTA).
-bool row2_ok(const FourStep &G) {
-    if (G.mode != ROW_CONV || G.c < 9 || G.c > 13) return false;
-    const uint32_t rows = 256u >> (G.c - 5);
-    return G.R % rows == 0;
-}
+// 2^9 .. 2^13 words).
+bool row2_ok(const FourStep &G) { return G.mode == ROW_CONV && G.c >= 9 && G.c <= 13; }
 
 cudaError_t launch_row2(const Primes3 &P3, const FourStep &G, const FSJobs &jobs, uint32_t njobs, cudaStream_t st) {
     const bool sq = G.square != 0;
