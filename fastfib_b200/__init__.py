@@ -279,6 +279,31 @@ def to_decimal(a, device_ptr: int = 0, n: int = 0):
     return s, True
 
 
+_SINK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+
+
+def to_decimal_stream(a):
+    """ffg_to_decimal_stream: (list of digit slices as str, True) from the
+    streamed device path, or ([], False) when it declined."""
+    pieces = []
+
+    def sink(ptr, n, user):
+        pieces.append(_ascii_str(ptr, n))
+
+    cb = _SINK(sink)
+    a = _arr(a)
+    nd, done = ctypes.c_size_t(), ctypes.c_int()
+    f = lib().ffg_to_decimal_stream
+    f.argtypes = [_u64p, ctypes.c_size_t, _SINK, ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                  ctypes.POINTER(ctypes.c_int)]
+    _check(f(a.ctypes.data_as(_u64p), a.size, cb, None, ctypes.byref(nd), ctypes.byref(done)))
+    if not done.value:
+        return [], False
+    if sum(len(x) for x in pieces) != nd.value:
+        raise FfgError("streamed digit count mismatch")
+    return pieces, True
+
+
 _decode_ascii = ctypes.pythonapi.PyUnicode_DecodeASCII
 _decode_ascii.restype = ctypes.py_object
 _decode_ascii.argtypes = [ctypes.c_void_p, ctypes.c_ssize_t, ctypes.c_char_p]

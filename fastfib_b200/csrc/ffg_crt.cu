@@ -35,6 +35,7 @@ constexpr uint32_t CRT_NL_MAX = 32 * 35;
 constexpr uint32_t CRT_NL_PER_W = 32;   // limbs per CTA = 32 * width
 
 FFG_DEV_INLINE int64_t floor_div(int64_t a, int64_t b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+FFG_DEV_INLINE int32_t floor_div32(int32_t a, int32_t b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
 FFG_DEV_INLINE uint32_t crt_ctas_dev(uint64_t nlimbs, uint32_t width) {
     const uint64_t NL = (uint64_t)CRT_NL_PER_W * width;
@@ -78,18 +79,35 @@ FFG_DEV_INLINE u128 garner(const GarnerConst &K, uint32_t r1, uint32_t r2, uint3
 
 // Column sum lo + 2^64 hi of limb j (relative to the CTA's first limb) over
 // the values Z_i 2^(i b) (i relative to the CTA's first coefficient, stored
-// from -halo), every Z_i below 2^(top + 1).
-FFG_DEV_INLINE void column_sum(const uint64_t *Zlo, const uint32_t *Zhi, int32_t j, uint32_t b, int32_t halo,
-                               int32_t top, uint64_t &s_lo, uint32_t &s_hi) {
-    const int64_t ilo = floor_div(64 * (int64_t)j - top + b - 1, b), ihi = floor_div(64 * (int64_t)j + 63, b);
+// from -halo), every Z_i below 2^(top + 1).  B: the width when known at
+// compile time (0: bw at run time); indices and shifts fit 32 bits (j is at
+// most 32 * 35 limbs, i at most 2048 + halo coefficients).
+template <int B>
+FFG_DEV_INLINE void column_sum_w(const uint64_t *Zlo, const uint32_t *Zhi, int32_t j, uint32_t bw, int32_t halo,
+                                 int32_t top, uint64_t &s_lo, uint32_t &s_hi) {
+    const int32_t b = B ? B : (int32_t)bw;
+    const int32_t ilo = floor_div32(64 * j - top + b - 1, b), ihi = floor_div32(64 * j + 63, b);
     s_lo = 0;
     s_hi = 0;
-    for (int64_t i = ilo < -halo ? -halo : ilo; i <= ihi; i++) {
+    for (int32_t i = ilo < -halo ? -halo : ilo; i <= ihi; i++) {
         const u128 X = ((u128)Zhi[i + halo] << 64) | Zlo[i + halo];
-        const int64_t sft = i * (int64_t)b - 64 * (int64_t)j;
+        const int32_t sft = i * b - 64 * j;
         const uint64_t part = sft >= 0 ? (uint64_t)(X << sft) : (uint64_t)(X >> (-sft));
         s_lo += part;
         s_hi += s_lo < part;
+    }
+}
+
+// The same with big_mul_ntt's widths (32..35) as compile-time divisors; b is
+// the same for every thread of a launch, so the switch does not diverge.
+FFG_DEV_INLINE void column_sum(const uint64_t *Zlo, const uint32_t *Zhi, int32_t j, uint32_t b, int32_t halo,
+                               int32_t top, uint64_t &s_lo, uint32_t &s_hi) {
+    switch (b) {
+    case 32: column_sum_w<32>(Zlo, Zhi, j, b, halo, top, s_lo, s_hi); return;
+    case 33: column_sum_w<33>(Zlo, Zhi, j, b, halo, top, s_lo, s_hi); return;
+    case 34: column_sum_w<34>(Zlo, Zhi, j, b, halo, top, s_lo, s_hi); return;
+    case 35: column_sum_w<35>(Zlo, Zhi, j, b, halo, top, s_lo, s_hi); return;
+    default: column_sum_w<0>(Zlo, Zhi, j, b, halo, top, s_lo, s_hi); return;
     }
 }
 

@@ -2387,8 +2387,18 @@ static int dec_prepare(int T, cudaStream_t st) {
 
 // The conversion proper; *err_flag set on the device when a correction fell
 // outside its range (the caller then converts on the host path).
+// Where a streamed conversion sends its digits (ffg_to_decimal_stream).
+struct DecSink {
+    ffg_digit_sink fn;
+    void *user;
+};
+
+static int dec_leaves_streamed(const LeafJob *dl, uint64_t nleaves, uint32_t chunks, uint64_t v, char *dd,
+                               const uint32_t *flags, int T, const DecSink &sink, size_t *nout, bool *fallback,
+                               cudaStream_t st);
+
 static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, size_t *nout, bool *fallback,
-                      cudaStream_t st) {
+                      cudaStream_t st, const DecSink *sink = nullptr) {
     *fallback = false;
     int T = 0;
     // powers as needed for the choice of T
@@ -2497,6 +2507,10 @@ static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, s
     int rc = dd ? dev_upload_jobs(lj.data(), lj.size() * sizeof(LeafJob), &dl, st) : fail(FFG_E_NOMEM, "digits");
     if (rc) return rc;
     const uint64_t v = (uint64_t)((~(u128h)0) / kDec19 - ((u128h)1 << 64));
+    if (sink) {
+        *out = nullptr;
+        return dec_leaves_streamed((const LeafJob *)dl, lj.size(), chunks, v, dd, flags, T, *sink, nout, fallback, st);
+    }
     cudaError_t e = launch_leaf_digits((const LeafJob *)dl, (uint32_t)lj.size(), chunks, v, dd, st);
     if (e) return fail(FFG_E_CUDA, "decimal leaves: %s", cudaGetErrorString(e));
     // leading zeros found on the device; only the digits cross to the host
@@ -2535,6 +2549,74 @@ static int dec_device(const uint64_t *x, uint64_t nx, uint64_t bx, char **out, s
     h[nd] = 0;
     *out = h;
     *nout = nd;
+    return FFG_OK;
+}
+
+// The leaves of a streamed conversion: the conversion's flags are read first
+// (a declined conversion emits nothing); then the leaves run in up to eight
+// launches, each followed by the copy of its digits into a pooled pinned
+// buffer and an event, and the host hands slice k to the sink (leading zeros
+// stripped) while the GPU still computes and copies the slices after it.
+static int dec_leaves_streamed(const LeafJob *dl, uint64_t nleaves, uint32_t chunks, uint64_t v, char *dd,
+                               const uint32_t *flags, int T, const DecSink &sink, size_t *nout, bool *fallback,
+                               cudaStream_t st) {
+    std::vector<uint32_t> hflags(2 * (T + 1));
+    CK(cudaMemcpyAsync(hflags.data(), flags, 8 * (T + 1), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int l = 0; l <= T; l++)
+        if (hflags[2 * l] || hflags[2 * l + 1]) {
+            g.err = "decimal conversion declined at level " + std::to_string(l) +
+                    (hflags[2 * l] ? ": quotient estimate out of range" : ": negative remainder");
+            *fallback = true;
+            return FFG_OK;
+        }
+    const uint64_t per = (uint64_t)chunks * 19, total = nleaves * per;
+    char *h = (char *)pinned_get(total);
+    if (!h) return fail(FFG_E_NOMEM, "host digits");
+    struct Guard {
+        char *h;
+        cudaStream_t st;
+        std::vector<cudaEvent_t> ev;
+        ~Guard() {
+            cudaStreamSynchronize(st);
+            for (auto e : ev)
+                if (e) cudaEventDestroy(e);
+            pinned_release(h);
+        }
+    } gd{h, st, {}};
+    const uint64_t K = nleaves < 8 ? nleaves : 8;
+    std::vector<uint64_t> cut(K + 1);
+    for (uint64_t k = 0; k <= K; k++) cut[k] = nleaves * k / K;
+    gd.ev.assign(K, nullptr);
+    for (uint64_t k = 0; k < K; k++) {
+        CK(cudaEventCreateWithFlags(&gd.ev[k], cudaEventDisableTiming));
+        const uint64_t j0 = cut[k], n = cut[k + 1] - cut[k];
+        cudaError_t e = launch_leaf_digits(dl + j0, (uint32_t)n, chunks, v, dd + j0 * per, st);
+        if (e) return fail(FFG_E_CUDA, "decimal leaves: %s", cudaGetErrorString(e));
+        CK(cudaMemcpyAsync(h + j0 * per, dd + j0 * per, n * per, cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(gd.ev[k], st));
+    }
+    ev_record(g.ev1, st);
+    size_t emitted = 0;
+    bool started = false;
+    for (uint64_t k = 0; k < K; k++) {
+        CK(cudaEventSynchronize(gd.ev[k]));
+        const char *p = h + cut[k] * per;
+        uint64_t n = (cut[k + 1] - cut[k]) * per;
+        if (!started) {
+            // the number is nonzero: its first digit is in some slice, and the
+            // slices of leading zeros before it emit nothing
+            uint64_t z = 0;
+            while (z < n && p[z] == '0') z++;
+            p += z, n -= z;
+            started = n > 0;
+        }
+        if (n) sink.fn(p, (size_t)n, sink.user);
+        emitted += (size_t)n;
+    }
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, g.ev0, g.ev1) == cudaSuccess) g_dec_ms = ms;
+    *nout = emitted;
     return FFG_OK;
 }
 
@@ -2599,6 +2681,49 @@ extern "C" int ffg_to_decimal_host(const uint64_t *x, size_t nx, char **out, siz
     cudaStreamSynchronize(g.stream);
     pinned_release(stage);
     return rc;
+}
+
+extern "C" int ffg_to_decimal_stream(const uint64_t *x, size_t nx, ffg_digit_sink sink, void *user, size_t *ndigits,
+                                     int *done) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!x || !sink || !ndigits || !done) return fail(FFG_E_ARG, "ffg_to_decimal_stream arguments");
+    while (nx > 1 && x[nx - 1] == 0) nx--;
+    *done = 0;
+    *ndigits = 0;
+    if (nx == 1 && x[0] == 0) return FFG_OK;
+    cudaStream_t st = g.stream;
+    CK(cudaStreamSynchronize(st));
+    arena_reset();
+    // the number gets the conversion's own buffer, kept between calls
+    if (g_dec_in_cap < nx) {
+        if (g_dec_in) cudaFree(g_dec_in);
+        g_dec_in = nullptr;
+        g_dec_in_cap = 0;
+        CK(cudaMalloc(&g_dec_in, nx * 8));
+        g_dec_in_cap = nx;
+    }
+    uint64_t *stage = (uint64_t *)pinned_get(nx * 8);
+    if (!stage) return fail(FFG_E_NOMEM, "pinned staging: %zu bytes", nx * 8);
+    memcpy(stage, x, nx * 8);
+    cudaError_t e = cudaMemcpyAsync(g_dec_in, stage, nx * 8, cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaStreamSynchronize(st);
+    pinned_release(stage);
+    if (e) return fail(FFG_E_CUDA, "decimal upload: %s", cudaGetErrorString(e));
+    uint64_t *dbits = (uint64_t *)arena_alloc(8), bx = 0;
+    if (!dbits) return fail(FFG_E_NOMEM, "device arena: bit length");
+    if ((e = launch_bit_length(g_dec_in, nx, dbits, st))) return fail(FFG_E_CUDA, "bit length: %s", cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(&bx, dbits, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (bx == 0) return FFG_OK;
+    bool fallback = false;
+    char *unused = nullptr;
+    const DecSink ds{sink, user};
+    rc = dec_device(g_dec_in, limbs_of(bx), bx, &unused, ndigits, &fallback, st, &ds);
+    if (rc) return rc;
+    *done = fallback ? 0 : 1;
+    return FFG_OK;
 }
 
 extern "C" double ffg_last_decimal_ms(void) { return g_dec_ms; }

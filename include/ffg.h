@@ -157,6 +157,19 @@ int ffg_time_batch(ffg_job *jobs, size_t count, int reps, double *ms);
    path). */
 int ffg_to_decimal_device(const uint64_t *x, size_t nx, char **out, size_t *nout, int *done);
 int ffg_to_decimal_host(const uint64_t *x, size_t nx, char **out, size_t *nout, int *done);
+
+/* big_to_string's output streamed (the command line's digit output,
+   src/main.c:88-102): the decimal digits of the host number x (nx limbs)
+   handed to sink in consecutive pieces, most significant first, leading zeros
+   dropped; each piece is valid only during its call.  The leaves of the
+   conversion run in slices, and a slice's digits go to the sink while the GPU
+   still computes and copies the ones after it.  *ndigits: the digits
+   emitted; *done 0 (nothing emitted) when the device path declined -- numbers
+   below 10^2432, or a correction out of range -- and the caller converts
+   another way (big_to_string).  Zero emits nothing, *done 0. */
+typedef void (*ffg_digit_sink)(const char *digits, size_t n, void *user);
+int ffg_to_decimal_stream(const uint64_t *x, size_t nx, ffg_digit_sink sink, void *user, size_t *ndigits,
+                          int *done);
 /* Device milliseconds of the last conversion's levels and leaves (CUDA
    events; the powers, reciprocals and copies excluded). */
 double ffg_last_decimal_ms(void);

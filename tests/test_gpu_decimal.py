@@ -78,3 +78,22 @@ def test_after_other_work(ff):
     for _ in range(2):
         assert hashlib.sha256(device_digits(ff, x).encode()).hexdigest() == gold["10000000"]
     assert ff.tickets_in_use() == 0
+
+
+def test_streamed_digits(ff):
+    """ffg_to_decimal_stream (the command line's streamed output): the slices
+    joined are the reference's digits of F(10^7) (hash), there is more than
+    one slice, and numbers whose top slices are all leading zeros stream
+    exactly str()'s digits."""
+    with open(GOLD) as f:
+        gold = json.load(f)
+    pieces, done = ff.to_decimal_stream(ff.fibonacci(10**7))
+    assert done and len(pieces) > 1
+    s = "".join(pieces)
+    assert len(s) == gold[f"digits_{10**7}"]
+    assert hashlib.sha256(s.encode()).hexdigest() == gold[str(10**7)]
+    for x in (10**(19 << 9) + 12345, (1 << 60000) + 1, 10**(38 << 8) - 1):
+        pieces, done = ff.to_decimal_stream(int_to_limbs(x))
+        assert done
+        assert "".join(pieces) == str(x)
+    assert ff.to_decimal_stream(int_to_limbs(12345)) == ([], False)  # below 10^2432: declined
