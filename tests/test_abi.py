@@ -18,6 +18,7 @@ def declared_functions():
             continue
         text = open(os.path.join(INC, fn)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"typedef[^;]*;", "", text)  # function-pointer types declare no symbol
         for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(", text, flags=re.M):
             name = m.group(1)
             if name not in ("if", "while", "for", "return", "sizeof"):
