@@ -459,6 +459,13 @@ def run_uneven(count=4096, reps=3, seed=4):
     torch.cuda.synchronize()
     pcie = {"h2d_ms": e0.elapsed_time(e1), "d2h_ms": e1.elapsed_time(e2)}
     del hin, hout, dbuf
+    # where the plain batch's device time goes: every launch bracketed by
+    # events, per kernel family (one extra call, outside the timed runs)
+    ff.profile(True)
+    ff.mul_batch_device([dict(j, method="plain") for j in jobs], stream)
+    torch.cuda.synchronize()
+    fam = {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in ff.profile_read().items() if v["launches"]}
+    ff.profile(False)
     # device-only times: the batch's launches captured once and replayed
     # (host planning outside the clock)
     graph_ms = {m: ff.time_batch([dict(j, method=m) for j in jobs], reps=3) for m in ("plain", "learned")}
@@ -475,7 +482,7 @@ def run_uneven(count=4096, reps=3, seed=4):
             "learned_vs_plain": res["plain"] / res["learned"],
             "batched_learned_vs_plain_unbatched": res["plain_unbatched"] / res["learned"],
             "e2e_ms": e2e, "h2d_bytes": in_bytes, "d2h_bytes": 8 * out_len, "pcie_copies_ms": pcie,
-            "graph_replay_device_ms": graph_ms,
+            "graph_replay_device_ms": graph_ms, "plain_families": fam,
             "timing": "plain / learned / unbatched: CUDA events on the call's stream around the whole call "
                       "(host planning included); graph_replay_device_ms: the launches alone; e2e_ms: the "
                       "host API with operands and products in host memory",
@@ -560,7 +567,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-f1e9", action="store_true", help="skip the extra F(10^9) measurement")
-    ap.add_argument("--config", default="fib", choices=["fib", "ntt", "ntt-suite", "uneven"],
+    ap.add_argument("--config", default="fib", choices=["fib", "ntt", "ntt-suite", "uneven", "decimal"],
                     help="fib: F(n) (the headline); ntt: one NTT product of --limbs limbs; "
                          "uneven: the uneven product stream, plain against learned dispatch")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-stream figures in the fib line")
@@ -583,6 +590,13 @@ def main():
         print(json.dumps({"metric": "NTT multiply ms (microbench: 2^14..2^22 limbs, squares and products, "
                                     "plan / forced 2^k / forced 3 2^k)", "unit": "ms", "higher_is_better": False,
                           "steps": args.steps, "warmup": args.warmup, "dtype": "u32", "config": r}), flush=True)
+        return 0 if r["bit_exact"] else 1
+    if args.config == "decimal":
+        import fastfib_b200 as ff
+        ff.set_device(0)
+        r = run_decimal(args.n, reps=args.steps)
+        print(json.dumps({"metric": "decimal conversion of F(n) ms (device)", "value": r["device_ms"], "unit": "ms",
+                          "higher_is_better": False, "steps": args.steps, "dtype": "u32", "config": r}), flush=True)
         return 0 if r["bit_exact"] else 1
     if args.config == "uneven":
         r = run_uneven(reps=args.steps)

@@ -132,6 +132,24 @@ def tune_geometry(lg_lo: int = 12, lg_hi: int = 24, reps: int = 5, log=None):
     return table
 
 
+def choice_gain_bound(raw) -> float:
+    """The most any per-product choice among the timed candidates could gain
+    over the reference's thresholds on the sampled shapes: sum over shapes of
+    the plain method's time over the sum of each shape's fastest candidate
+    (schoolbook below a short side of 200 limbs, the NTT plan from there, as
+    the reference's dispatch, src/mul_basic.c:30-38)."""
+    by = {}
+    for ba, bb, sq, name, us in raw:
+        by.setdefault((ba, bb, sq), {})[name] = us
+    plain = best = 0.0
+    for (ba, bb, sq), t in by.items():
+        short = min((ba + 63) // 64, (bb + 63) // 64)
+        p = t["ntt"] if short >= 200 or "school" not in t else t["school"]
+        plain += p
+        best += min(t.values())
+    return plain / best if best else 1.0
+
+
 def fit(X, M, Y, epochs: int = 2000, lr: float = 1e-2, seed: int = 0):
     params, hist = ff.mlp_train(ff.mlp_init(seed), X, M, Y, epochs=epochs, lr=lr)
     return params, hist
@@ -160,7 +178,8 @@ def main(argv=None):
     rms = float(np.sqrt(np.mean((pred - Y) ** 2)))
     meta = {"rows": int(len(Y)), "shapes": args.shapes, "seed": args.seed, "epochs": args.epochs, "lr": args.lr,
             "loss_first": float(hist[0]), "loss_last": float(hist[-1]), "rms_log2_error": rms,
-            "geometry_rows": len(geometry), "geometry_s": round(t1 - t0, 1), "collect_s": round(t2 - t1, 1),
+            "geometry_rows": len(geometry), "choice_gain_bound": round(choice_gain_bound(raw), 4),
+            "geometry_s": round(t1 - t0, 1), "collect_s": round(t2 - t1, 1),
             "train_s": round(time.time() - t2, 1)}
     try:
         import torch
