@@ -82,6 +82,73 @@ FFG_DEV_INLINE uint32_t digit_res(const uint64_t *__restrict__ src, uint64_t ns,
 // The digit of row r, column n2 of the operand's four-step layout.
 #define FFG_COL_DIGIT(r) digit_res<PI>(src, ns, cs, off, w, (uint64_t)(r) * C + c0 + c, P)
 
+// What the first step of a forward column tile reads: the operand's digits.
+struct ColSrc {
+    const uint64_t *src;
+    uint64_t ns, cs, off;
+    uint32_t w, C, c0, wc, wlg, LS;
+};
+
+// The first step of a power-of-two forward column tile, straight from the
+// digits, when only rows below NZ * (its stride) can be nonzero (a product's
+// operands fill at most the lower half of the transform, a short operand much
+// less): the zero slots are neither read nor transformed (dft_dif_nz).
+// Step A (radix 2^MA at stride 2^RN / 2^MA) when MA > 0, else step B (radix
+// 2^MB at stride 32, one block).
+template <int PI, int RN, int NZ>
+FFG_DEV_INLINE void col_fwd2_first(const PrimeDev &P, const ColSrc &S, uint32_t *smem) {
+    using Q = ColGeo<RN>;
+    const uint64_t *src = S.src;
+    const uint64_t ns = S.ns, cs = S.cs, off = S.off;
+    const uint32_t w = S.w, C = S.C, c0 = S.c0, wc = S.wc, wlg = S.wlg, LS = S.LS;
+    if (Q::MA) {
+        const uint2 *tw = P.stw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
+        const uint32_t slots = wc * Q::SA;
+#pragma unroll 1
+        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
+            const uint32_t c = s & (wc - 1), j = s >> wlg;
+            uint32_t *d = smem + c * LS + j + (j >> 5);
+            uint32_t x[Q::RA];
+#pragma unroll
+            for (uint32_t t = 0; t < Q::RA; t++) x[t] = t < (uint32_t)NZ ? FFG_COL_DIGIT(j + Q::SA * t) : 0u;
+            dft_dif_nz<PI, Q::MA, NZ>(x);
+#pragma unroll
+            for (uint32_t t = 1; t < Q::RA; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * Q::SA + j]));
+#pragma unroll
+            for (uint32_t t = 0; t < Q::RA; t++) d[t * Q::SAP] = x[t];
+        }
+    } else {
+        const uint2 *tw = P.stw + c_lines.tw_off[5 * 6 + Q::MB];
+        const uint32_t slots = wc * 32;
+#pragma unroll 1
+        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
+            const uint32_t c = s & (wc - 1), j = s >> wlg;
+            uint32_t *d = smem + c * LS + j;
+            uint32_t x[Q::RB];
+#pragma unroll
+            for (uint32_t t = 0; t < Q::RB; t++) x[t] = t < (uint32_t)NZ ? FFG_COL_DIGIT(j + 32 * t) : 0u;
+            dft_dif_nz<PI, Q::MB, NZ>(x);
+#pragma unroll
+            for (uint32_t t = 1; t < Q::RB; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * 32 + j]));
+#pragma unroll
+            for (uint32_t t = 0; t < Q::RB; t++) d[33 * t] = x[t];
+        }
+    }
+}
+
+// col_fwd2_first for the least power of two NZ covering nzt slots.
+template <int PI, int RN>
+FFG_DEV_INLINE void col_fwd2_first_any(const PrimeDev &P, const ColSrc &S, uint32_t *smem, uint32_t nzt) {
+    using Q = ColGeo<RN>;
+    constexpr int M = Q::MA ? Q::MA : Q::MB;
+    if (nzt <= 1) col_fwd2_first<PI, RN, 1>(P, S, smem);
+    else if (nzt <= 2 || M < 2) col_fwd2_first<PI, RN, (M >= 1 ? 2 : 1)>(P, S, smem);
+    else if (nzt <= 4 || M < 3) col_fwd2_first<PI, RN, (M >= 2 ? 4 : 1)>(P, S, smem);
+    else if (nzt <= 8 || M < 4) col_fwd2_first<PI, RN, (M >= 3 ? 8 : 1)>(P, S, smem);
+    else if (nzt <= 16 || M < 5) col_fwd2_first<PI, RN, (M >= 4 ? 16 : 1)>(P, S, smem);
+    else col_fwd2_first<PI, RN, (M >= 5 ? 32 : 1)>(P, S, smem);
+}
+
 template <int PI, int RN, bool R3>
 FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FSJob &J, uint32_t *smem) {
     using Q = ColGeo<RN>;
@@ -109,7 +176,18 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
         }
         __syncthreads();
     }
-    if (Q::MA) {
+    if (!R3) {
+        // rows at or past rows_nz are zero in every column of the tile
+        const uint64_t avail = (ns * 64 + w - 1) / w; // digits that start inside the limbs
+        const uint64_t lim = cs < (avail > off ? avail - off : 0) ? cs : (avail > off ? avail - off : 0);
+        const uint64_t rows_nz = lim > c0 ? (lim - c0 + C - 1) / C : 0;
+        const uint32_t stride = Q::MA ? Q::SA : 32;
+        const uint32_t nzt = (uint32_t)((rows_nz + stride - 1) / stride);
+        const ColSrc S{src, ns, cs, off, w, C, c0, wc, wlg, LS};
+        col_fwd2_first_any<PI, RN>(P, S, smem, nzt);
+        __syncthreads();
+    }
+    if (Q::MA && R3) {
         const uint2 *tw = P.stw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
         const uint32_t slots = wc * NBLK * Q::SA;
 #pragma unroll 1
@@ -118,7 +196,7 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
             uint32_t *d = smem + c * LS + q * BP + j + (j >> 5);
             uint32_t x[Q::RA];
 #pragma unroll
-            for (uint32_t t = 0; t < Q::RA; t++) x[t] = R3 ? d[t * Q::SAP] : FFG_COL_DIGIT(j + Q::SA * t);
+            for (uint32_t t = 0; t < Q::RA; t++) x[t] = d[t * Q::SAP];
             dft_dif<PI, Q::MA>(x);
 #pragma unroll
             for (uint32_t t = 1; t < Q::RA; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * Q::SA + j]));
@@ -127,7 +205,7 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
         }
         __syncthreads();
     }
-    {
+    if (Q::MA || R3) {
         const uint2 *tw = P.stw + c_lines.tw_off[5 * 6 + Q::MB];
         const uint32_t slots = wc * NBLK * (Q::R / Q::RB);
 #pragma unroll 1
@@ -137,8 +215,7 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
             uint32_t *d = smem + c * LS + b * Q::NBP + j;
             uint32_t x[Q::RB];
 #pragma unroll
-            for (uint32_t t = 0; t < Q::RB; t++)
-                x[t] = (Q::MA || R3) ? d[33 * t] : FFG_COL_DIGIT(b * Q::NB + j + 32 * t);
+            for (uint32_t t = 0; t < Q::RB; t++) x[t] = d[33 * t];
             dft_dif<PI, Q::MB>(x);
 #pragma unroll
             for (uint32_t t = 1; t < Q::RB; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * 32 + j]));

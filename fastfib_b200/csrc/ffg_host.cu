@@ -419,13 +419,17 @@ static bool geo_valid(uint32_t lg, uint32_t r3, uint32_t c, uint32_t wc) {
 }
 
 static void gpu_geometry(ffg_plan *pl) {
-    if (pl->L <= kSmallMaxL && !pl->split) {
+    const Geo &t = g_geo[pl->lg & 31][pl->r3 ? 1 : 0];
+    const bool tuned = t.set && geo_valid(pl->lg, pl->r3, t.c, t.wc);
+    // short lengths run the one-CTA transform, unless the autotuner measured
+    // a four-step geometry faster for this length (a single product or a
+    // doubling step's pair gives the one-CTA kernel only six CTAs)
+    if (pl->L <= kSmallMaxL && !pl->split && !tuned) {
         pl->kernel = 0;
         pl->row_lg = 0;
         return;
     }
-    const Geo &t = g_geo[pl->lg & 31][pl->r3 ? 1 : 0];
-    if (t.set && geo_valid(pl->lg, pl->r3, t.c, t.wc)) {
+    if (tuned) {
         pl->kernel = 1;
         pl->row_lg = t.c;
         return;

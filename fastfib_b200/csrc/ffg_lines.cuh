@@ -84,6 +84,33 @@ FFG_DEV_INLINE void dft_dif(uint32_t (&x)[1 << M]) {
     }
 }
 
+// dft_dif for inputs whose slots t >= NZ are zero (NZ a power of two; the
+// caller sets them to the constant 0).  While the half distance h is at
+// least NZ a level's partner is zero, so (a, 0) -> (a, a w): the level costs
+// only the multiplications of its nonzero slots, and all-zero pairs are
+// skipped; once h < NZ every slot is live and the levels are dft_dif's.
+template <int PI, int M, int NZ>
+FFG_DEV_INLINE void dft_dif_nz(uint32_t (&x)[1 << M]) {
+    constexpr uint32_t p = kPrimeC[PI];
+#pragma unroll
+    for (int l = 0; l < M; l++) {
+        const int h = 1 << (M - 1 - l);
+#pragma unroll
+        for (int t = 0; t < (1 << M); t++) {
+            if (t & h) continue;
+            const int e = (t & (h - 1)) * (16 / h);
+            if (h >= NZ) {
+                if ((t & (h - 1)) >= NZ) continue; // both slots still zero
+                x[t + h] = e ? sh<PI>(x[t], c_lines.f[PI][e]) : x[t];
+            } else {
+                const uint32_t a = x[t], b = x[t + h];
+                x[t] = ad<PI>(a, b);
+                x[t + h] = e ? sh<PI>(a - b + p, c_lines.f[PI][e]) : sb<PI>(a, b);
+            }
+        }
+    }
+}
+
 // The inverse: decimation in time, bit-reversed in, natural out, 2^M times
 // the inverse DFT.
 template <int PI, int M>

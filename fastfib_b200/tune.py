@@ -96,17 +96,17 @@ def collect(shapes, reps: int = 3, log=None):
     return np.array(X, np.float32), np.array(M, np.int32), np.array(Y, np.float32), raw
 
 
-def tune_geometry(lg_lo: int = 12, lg_hi: int = 24, reps: int = 5, log=None):
-    """Per transform length (2^lg and 3 2^lg past the one-CTA kernel's 4096)
-    the fastest (row_lg, wc) on two squarings of about 0.9 L coefficients at
-    a time, the fast-doubling chain's pair (device time of graph replays).
-    Returns the rows installed."""
+def tune_geometry(lg_lo: int = 10, lg_hi: int = 24, reps: int = 5, log=None):
+    """Per transform length (2^lg and 3 2^lg from 1024; up to 4096 against
+    the one-CTA kernel, the default there) the fastest (row_lg, wc) on two
+    squarings of about 0.9 L coefficients at a time, the fast-doubling
+    chain's pair (device time of graph replays).  Returns the rows installed."""
     table = []
     cap = ff.ntt_max_L()
     for lg in range(lg_lo, lg_hi + 1):
         for r3 in (0, 1):
             L = (3 if r3 else 1) << lg
-            if L <= 4096 or L > cap:
+            if L < 1024 or L > cap:  # up to 4096 the default is the one-CTA transform
                 continue
             bits = int(0.9 * L * 32 / 2)
             method = "ntt_r3" if r3 else "ntt_pow2"

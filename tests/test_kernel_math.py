@@ -204,3 +204,44 @@ def test_fingerprint_runs():
                         h = h * pow(r64, i0, p) % p
                     total = (total + h) % p
                 assert total == x % p, (n, nthreads, p)
+
+
+def _dif(x, p, w32, nz=None):
+    """The in-register radix-2^M decimation in frequency of ffg_lines.cuh
+    (dft_dif), or with nz set its pruned form for inputs zero at slots >= nz
+    (dft_dif_nz): while the half distance h >= nz a pair (a, 0) becomes
+    (a, a w) and all-zero pairs are skipped."""
+    x = list(x)
+    n = len(x)
+    M = n.bit_length() - 1
+    for lev in range(M):
+        h = 1 << (M - 1 - lev)
+        for t in range(n):
+            if t & h:
+                continue
+            e = (t & (h - 1)) * (16 // h)
+            w = pow(w32, e, p)
+            if nz is not None and h >= nz:
+                if (t & (h - 1)) >= nz:
+                    continue
+                x[t + h] = x[t] * w % p
+            else:
+                a, b = x[t], x[t + h]
+                x[t], x[t + h] = (a + b) % p, (a - b) * w % p
+    return x
+
+
+def test_pruned_dif_matches_full():
+    """The first column step's zero-row pruning (ffg_cols.cu col_fwd2_first,
+    dft_dif_nz): for every radix 2..32 and every power-of-two count of
+    nonzero leading slots, the pruned transform equals the full one."""
+    rng = random.Random(5)
+    for p, g in ((2113929217, 5), (2013265921, 31), (1811939329, 13)):
+        w32 = pow(g, (p - 1) // 32, p)
+        for M in range(1, 6):
+            n = 1 << M
+            for k in range(M + 1):
+                nz = 1 << k
+                for _ in range(20):
+                    x = [rng.randrange(p) if t < nz else 0 for t in range(n)]
+                    assert _dif(x, p, w32, nz) == _dif(x, p, w32)
