@@ -709,10 +709,18 @@ def main():
     if rank == 0:
         peak, peak_src = hbm_peak()
         achieved = prof["bytes"] / (prof["ms"] * 1e-3) / 1e9 if prof["ms"] > 0 else 0.0
-        traffic = None
+        traffic, compute = None, None
         if os.path.exists(TRAFFIC):
             with open(TRAFFIC) as f:
-                traffic = json.load(f).get(dominant, {}).get("dram_bytes_per_launch")
+                tr = json.load(f)
+            fam = tr.get(dominant, {})
+            traffic = fam.get("dram_bytes_per_launch")
+            if "issue_active_pct" in fam:
+                # what binds the kernel: the integer pipes' issue, from the same
+                # ncu capture as the traffic (committed under profiles/)
+                compute = {k: fam[k] for k in ("issue_active_pct", "alu_pipe_pct", "fma_pipe_pct",
+                                               "warps_active_pct") if k in fam}
+                compute["source"] = tr.get("source")
         line = {
             "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
@@ -724,9 +732,12 @@ def main():
                          "traffic": traffic, "launches": prof["launches"],
                          "algorithmic_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]),
                          "ms_per_launch": prof["ms"] / max(1, prof["launches"]),
-                         "note": "modular integer transforms: the integer ALU pipe, not HBM, binds them "
-                                 "(51-67 % busy at L = 2^24, profiles/ntt_l2e24_sections.md); at F(10^8) "
-                                 "most launches are also short enough to be latency-bound"},
+                         "compute": compute,
+                         "note": "exact modular integer transforms: instruction issue on the integer ALU and "
+                                 "FMA pipes binds them, not HBM (compute: ncu fractions of peak for this "
+                                 "kernel family in the F(10^8) chain); the arithmetic alone caps the NTT "
+                                 "passes at about 52 % of HBM (profiles/ntt_l2e24.md); at F(10^8) the middle "
+                                 "steps are short launches bound by latency"},
             "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": clk.summary(),
