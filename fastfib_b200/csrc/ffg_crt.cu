@@ -65,6 +65,22 @@ __global__ void __launch_bounds__(CRT_THREADS) k_crt_batch(GarnerConst K, const 
     crt_block(K, J, blockIdx.x);
 }
 
+// CRTs of any sizes in one launch: CTA b runs CTA b - first[j] of job j,
+// first[j] <= b < first[j + 1] (first: count + 1 prefix sums of the jobs'
+// CTA counts), found by binary search.
+__global__ void __launch_bounds__(CRT_THREADS) k_crt_flat(GarnerConst K, const CrtJob *__restrict__ jobs,
+                                                         const uint32_t *__restrict__ first, uint32_t count) {
+    const uint32_t b = blockIdx.x;
+    uint32_t lo = 0, hi = count; // invariant: first[lo] <= b < first[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (__ldg(&first[mid]) <= b) lo = mid;
+        else hi = mid;
+    }
+    const CrtJob J = jobs[lo];
+    crt_block(K, J, b - __ldg(&first[lo]));
+}
+
 // Garner's recombination of one coefficient's residues: X < p1 p2 p3 < 2^93.
 FFG_DEV_INLINE u128 garner(const GarnerConst &K, uint32_t r1, uint32_t r2, uint32_t r3) {
     const uint32_t p1 = K.p[0], p2 = K.p[1], p3 = K.p[2];
@@ -99,7 +115,7 @@ FFG_DEV_INLINE void column_sum_w(const uint64_t *Zlo, const uint32_t *Zhi, int32
 }
 
 // The same with big_mul_ntt's widths (32..35) as compile-time divisors; b is
-// the same for every thread of a launch, so the switch does not diverge.
+// the same for every thread of a CTA, so the switch does not diverge.
 FFG_DEV_INLINE void column_sum(const uint64_t *Zlo, const uint32_t *Zhi, int32_t j, uint32_t b, int32_t halo,
                                int32_t top, uint64_t &s_lo, uint32_t &s_hi) {
     switch (b) {
@@ -250,6 +266,21 @@ cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_
     if (!count) return cudaSuccess;
     prof_begin(PK_CRT, st);
     k_crt_batch<<<dim3(max_ctas, count), CRT_THREADS, crt_smem(), st>>>(garner_const(), d_jobs);
+    prof_end(PK_CRT, st, bytes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt_flat(const CrtJob *d_jobs, const uint32_t *d_first, uint32_t count, uint32_t total_ctas,
+                            cudaStream_t st, double bytes) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_crt_flat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)crt_smem());
+        if (e) return e;
+        configured = true;
+    }
+    if (!count || !total_ctas) return cudaSuccess;
+    prof_begin(PK_CRT, st);
+    k_crt_flat<<<total_ctas, CRT_THREADS, crt_smem(), st>>>(garner_const(), d_jobs, d_first, count);
     prof_end(PK_CRT, st, bytes);
     return cudaGetLastError();
 }

@@ -1317,7 +1317,11 @@ struct GroupKey {
     }
 };
 
-static const uint64_t kBatchSmallMaxL = 16384; // longest line one CTA holds (FFG_LINE_LG)
+// longest line one CTA holds (FFG_LINE_LG); measured: with the fixed-shape
+// four-step passes, groups of 64+ products up to this length still run
+// faster as one CTA per product and prime (the decimal conversion of F(10^8):
+// 14.2 ms, against 15.1 / 17.8 ms with the bound at 8192 / 4096)
+static const uint64_t kBatchSmallMaxL = 16384;
 static const size_t kBatchSmallMin = 64;       // products of one plan (a decimal level has hundreds)
 
 // Runs a batch: one schoolbook launch for every schoolbook product, then per
@@ -1376,12 +1380,16 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capt
     };
     struct Launch {
         GroupKey key;
-        size_t conv_off, crt_off, count;
-        uint32_t crt_ctas_max;
-        double conv_bytes, crt_bytes;
+        size_t conv_off, count;
+        double conv_bytes;
         ffg_plan pl;
     };
     std::vector<Launch> launches;
+    // every group's CRTs, run after all transforms as one launch (k_crt_flat:
+    // first[j] is the first CTA of CRT j)
+    std::vector<CrtJob> crts;
+    std::vector<uint32_t> crt_first{0};
+    double crt_bytes = 0;
     size_t school_off = sj.empty() ? 0 : put(sj.data(), sj.size() * sizeof(SchoolJob));
     for (auto &kv : groups) {
         const GroupKey &k = kv.first;
@@ -1390,10 +1398,9 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capt
         const uint32_t w = pl.width;
         std::vector<ConvJob> cj;
         std::vector<FSJob> fj;
-        std::vector<CrtJob> rj;
         uint32_t scl[3], scls[3];
         scale_consts(L, scl, scls);
-        Launch ln{k, 0, 0, kv.second.size(), 0, 0, 0, pl};
+        Launch ln{k, 0, kv.second.size(), 0, pl};
         for (size_t idx : kv.second) {
             BJob &J = jobs[idx];
             uint32_t *ya = (uint32_t *)arena_alloc(3 * L * sizeof(uint32_t));
@@ -1421,14 +1428,15 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capt
             r.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(r.nlimbs, w) * 4);
             if (!r.maps) return fail(FFG_E_NOMEM, "device arena: batch carry maps");
             r.ticket = ticket_get();
-            ln.crt_ctas_max = std::max(ln.crt_ctas_max, crt_ctas(r.nlimbs, w));
-            ln.crt_bytes += 12.0 * (double)r.conv + 8.0 * (double)r.nlimbs;
-            rj.push_back(r);
+            crt_bytes += 12.0 * (double)r.conv + 8.0 * (double)r.nlimbs;
+            crt_first.push_back(crt_first.back() + crt_ctas(r.nlimbs, w));
+            crts.push_back(r);
         }
         ln.conv_off = k.kernel == 0 ? put(cj.data(), cj.size() * sizeof(ConvJob)) : put(fj.data(), fj.size() * sizeof(FSJob));
-        ln.crt_off = put(rj.data(), rj.size() * sizeof(CrtJob));
         launches.push_back(ln);
     }
+    const size_t crt_off = crts.empty() ? 0 : put(crts.data(), crts.size() * sizeof(CrtJob));
+    const size_t first_off = crts.empty() ? 0 : put(crt_first.data(), crt_first.size() * sizeof(uint32_t));
     char *dimg = nullptr;
     if (!img.empty()) {
         dimg = (char *)arena_alloc(img.size());
@@ -1481,12 +1489,11 @@ static int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capt
                 if (e) return end_capture(fail(FFG_E_CUDA, "batched four-step: %s", cudaGetErrorString(e)));
             }
         }
-        for (size_t base = 0; base < ln.count; base += 65535) {
-            const uint32_t cnt = (uint32_t)std::min<size_t>(65535, ln.count - base);
-            e = launch_crt_batch((const CrtJob *)(dimg + ln.crt_off) + base, cnt, ln.crt_ctas_max, st,
-                                 ln.crt_bytes * cnt / ln.count);
-            if (e) return end_capture(fail(FFG_E_CUDA, "batched CRT: %s", cudaGetErrorString(e)));
-        }
+    }
+    if (!crts.empty()) {
+        e = launch_crt_flat((const CrtJob *)(dimg + crt_off), (const uint32_t *)(dimg + first_off),
+                            (uint32_t)crts.size(), crt_first.back(), st, crt_bytes);
+        if (e) return end_capture(fail(FFG_E_CUDA, "batched CRT: %s", cudaGetErrorString(e)));
     }
     for (size_t idx : splits) {
         BJob &J = jobs[idx];

@@ -213,6 +213,10 @@ __host__ __device__ uint32_t school_ctas(uint64_t nlimbs); // CTAs (and carry ma
 // Batches in device arrays: one launch (plus one settle) for all products.
 cudaError_t launch_crt_batch(const CrtJob *d_jobs, uint32_t count, uint32_t max_ctas, cudaStream_t st,
                              double bytes);
+// CRTs of different sizes in one launch of total_ctas CTAs: d_first holds the
+// count + 1 prefix sums of the jobs' crt_ctas.
+cudaError_t launch_crt_flat(const CrtJob *d_jobs, const uint32_t *d_first, uint32_t count, uint32_t total_ctas,
+                            cudaStream_t st, double bytes);
 cudaError_t launch_school_pair(const SchoolJob *jobs, uint32_t count, cudaStream_t st);
 // The doubling step's two short squarings (a == b), SQ_NL output limbs per
 // CTA: school_sq_ctas(nlimbs) words of maps each.
