@@ -362,8 +362,16 @@ def run_decimal(n=10**8, reps=3):
     with open(os.path.join(ROOT, "tests", "golden", "decimal_sha256.json")) as fh:
         gold = json.load(fh)
     ok = bool(done) and str(n) in gold and hashlib.sha256(s.encode()).hexdigest() == gold[str(n)]
+    # where the conversion's device time goes: one more call with every launch
+    # bracketed by events, per kernel family (the decimal kernels of
+    # ffg_decimal.cu count under "lin"; events perturb short launches)
+    ff.profile(True)
+    ff.to_decimal(f)
+    fam = {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in ff.profile_read().items() if v["launches"]}
+    ff.profile(False)
     return {"n": n, "digits": len(s) if s else 0, "device_ms": statistics.median(dev),
             "e2e_ms": statistics.median(wall), "uncached_e2e_ms": first, "device_path": bool(done), "bit_exact": ok,
+            "families": fam,
             "note": "device_ms / e2e_ms: powers of ten and reciprocals cached from an earlier call; "
                     "uncached_e2e_ms: recomputed inside the call, as the reference's big_to_string does"}
 
@@ -419,10 +427,10 @@ def run_uneven(count=4096, reps=3, seed=4):
     stream = ts_stream.cuda_stream
     res = {}
     for m in ("plain", "learned"):
-        js = [dict(j, method=m) for j in jobs]
+        js = ff.device_jobs([dict(j, method=m) for j in jobs])  # job records built once, outside the clock
         res[m] = timed(lambda: ff.mul_batch_device(js, stream))
-    js = [dict(j, method="plain") for j in jobs]
-    res["plain_unbatched"] = timed(lambda: [ff.mul_batch_device([j], stream) for j in js])
+    js = ff.device_jobs([dict(j, method="plain") for j in jobs])
+    res["plain_unbatched"] = timed(lambda: [ff.mul_batch_device(js[i:i + 1], stream) for i in range(len(js))])
     # correctness of the learned run (the last one executed above was plain
     # unbatched; run learned once more and check every product)
     ff.mul_batch_device([dict(j, method="learned") for j in jobs], stream)

@@ -372,9 +372,36 @@ def mul_batch(pairs, method="ntt") -> list:
     return [area[offs[i]: offs[i] + jobs[i].nout] for i in range(len(pairs))]
 
 
+# ffg_job as a numpy record (the same 72-byte layout as Job)
+_JOB_DT = np.dtype([("a", "<u8"), ("b", "<u8"), ("na", "<u8"), ("nb", "<u8"), ("bits_a", "<u8"),
+                    ("bits_b", "<u8"), ("out", "<u8"), ("nout", "<u8"), ("square", "<i4"), ("method", "<i4")])
+
+
+def device_jobs(jobs) -> np.ndarray:
+    """The job records of mul_batch_device (a list of dicts as it takes) built
+    column by column, to be reused across calls."""
+    arr = np.zeros(len(jobs), dtype=_JOB_DT)
+    arr["a"] = [d["a"] for d in jobs]
+    arr["b"] = [d.get("b") or d["a"] for d in jobs]
+    arr["na"] = [d["na"] for d in jobs]
+    arr["nb"] = [d.get("nb", d["na"]) for d in jobs]
+    arr["bits_a"] = [d["bits_a"] for d in jobs]
+    arr["bits_b"] = [d.get("bits_b", d["bits_a"]) for d in jobs]
+    arr["out"] = [d["out"] for d in jobs]
+    arr["square"] = [int(d.get("square", False)) for d in jobs]
+    arr["method"] = [METHODS[d.get("method", "ntt")] for d in jobs]
+    return arr
+
+
 def mul_batch_device(jobs, stream: int = 0) -> None:
     """ffg_mul_batch_device on a list of dicts with device pointers:
-    a, b, na, nb, bits_a, bits_b, out (na + nb + 1 limbs), square, method."""
+    a, b, na, nb, bits_a, bits_b, out (na + nb + 1 limbs), square, method --
+    or on the records device_jobs built from such a list."""
+    if isinstance(jobs, np.ndarray):
+        assert jobs.dtype == _JOB_DT
+        ptr = ctypes.cast(jobs.ctypes.data, ctypes.POINTER(Job))
+        _check(lib().ffg_mul_batch_device(ptr, len(jobs), stream or None))
+        return
     _check(lib().ffg_mul_batch_device(_device_jobs(jobs), len(jobs), stream or None))
 
 

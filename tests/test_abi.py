@@ -113,3 +113,11 @@ def test_small_decimal_on_the_host(ff):
     for x in xs:
         assert x.bit_length() < 16384
         assert ff.big_to_string(int_to_limbs(x)) == str(x), x.bit_length()
+
+
+def test_job_records_match_the_struct(ff):
+    """device_jobs builds the same bytes as the ffg_job structs (include/ffg.h)."""
+    jobs = [{"a": 1000 + i, "b": None if i % 3 == 0 else 2000 + i, "na": 100 + i, "nb": 200, "bits_a": 6400 + i,
+             "bits_b": 12800, "out": 3000 + i, "square": i % 3 == 0, "method": ("plain", "ntt", "learned")[i % 3]}
+            for i in range(50)]
+    assert bytes(ff._device_jobs(jobs)) == ff.device_jobs(jobs).tobytes()
