@@ -347,29 +347,30 @@ def mul(a, b=None) -> np.ndarray:
 def mul_batch(pairs, method="ntt") -> list:
     """ffg_mul_batch_host: many independent products in one call.  pairs holds
     (a, b) with b None for a square; method names one of METHODS, or is a list
-    with one name per product."""
-    arrs, jobs = [], (Job * max(1, len(pairs)))()
-    # one output area for the whole batch (written only where the products
-    # land); each result is a view of its part
-    sizes = [(_arr(a).size, (_arr(a) if b is None else _arr(b)).size) for a, b in pairs]
-    area = np.empty(sum(x + y for x, y in sizes), dtype=np.uint64)
-    base = area.ctypes.data
-    offs, o = [], 0
-    for i, (a, b) in enumerate(pairs):
-        a = _arr(a)
-        sq = b is None
-        b = a if sq else _arr(b)
-        arrs += [a, b]
-        offs.append(o)
-        m = method[i] if isinstance(method, (list, tuple)) else method
-        j = jobs[i]
-        j.a, j.b = a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p)
-        j.na, j.nb = a.size, b.size
-        j.out = ctypes.cast(base + 8 * o, _u64p)
-        j.square, j.method = int(sq), METHODS[m]
-        o += a.size + b.size
-    _check(lib().ffg_mul_batch_host(jobs, len(pairs)))
-    return [area[offs[i]: offs[i] + jobs[i].nout] for i in range(len(pairs))]
+    with one name per product.  The products come back as views of one
+    output area."""
+    A = [_arr(a) for a, _ in pairs]
+    B = [A[i] if b is None else _arr(b) for i, (_, b) in enumerate(pairs)]
+    n = len(pairs)
+    jobs = np.zeros(max(1, n), dtype=_JOB_DT)
+    if n:
+        na = np.fromiter((a.size for a in A), dtype=np.uint64, count=n)
+        nb = np.fromiter((b.size for b in B), dtype=np.uint64, count=n)
+        offs = np.concatenate([[0], np.cumsum(na + nb)[:-1]]).astype(np.uint64)
+        area = np.empty(int((na + nb).sum()), dtype=np.uint64)
+        jobs["a"][:n] = [a.ctypes.data for a in A]
+        jobs["b"][:n] = [b.ctypes.data for b in B]
+        jobs["na"][:n], jobs["nb"][:n] = na, nb
+        jobs["out"][:n] = area.ctypes.data + 8 * offs
+        jobs["square"][:n] = [int(b is None) for _, b in pairs]
+        ms = method if isinstance(method, (list, tuple)) else [method] * n
+        jobs["method"][:n] = [METHODS[m] for m in ms]
+    ptr = ctypes.cast(jobs.ctypes.data, ctypes.POINTER(Job))
+    _check(lib().ffg_mul_batch_host(ptr, n))
+    if not n:
+        return []
+    nout = jobs["nout"]
+    return [area[int(offs[i]): int(offs[i]) + int(nout[i])] for i in range(n)]
 
 
 # ffg_job as a numpy record (the same 72-byte layout as Job)
