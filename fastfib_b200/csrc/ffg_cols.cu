@@ -89,51 +89,103 @@ struct ColSrc {
     uint32_t w, C, c0, wc, wlg, LS;
 };
 
+// The raw limb words behind one digit: the 32-bit word itself for 32-bit
+// digits, else the two 64-bit limbs the digit may straddle.
+template <bool W32> struct DigitRaw;
+template <> struct DigitRaw<true> {
+    uint32_t v;
+    FFG_DEV_INLINE void fetch(const ColSrc &S, uint64_t i, bool ok) {
+        // digit i is 32-bit word off + i of the limbs
+        const uint64_t q = S.off + i;
+        v = ok && i < S.cs && (q >> 1) < S.ns ? __ldg((const uint32_t *)S.src + q) : 0u;
+    }
+    template <int PI> FFG_DEV_INLINE uint32_t residue(const ColSrc &, uint64_t, const PrimeDev &) const {
+        constexpr uint32_t p = kPrimeC[PI];
+        uint32_t l = v;
+        l = min(l, l - p);
+        return min(l, l - p);
+    }
+};
+template <> struct DigitRaw<false> {
+    uint64_t lo, hi;
+    FFG_DEV_INLINE void fetch(const ColSrc &S, uint64_t i, bool ok) {
+        const uint64_t bit = (S.off + i) * S.w, q = bit >> 6;
+        const uint32_t sft = (uint32_t)(bit & 63);
+        ok = ok && i < S.cs;
+        lo = ok && q < S.ns ? __ldg(&S.src[q]) : 0;
+        hi = ok && sft + S.w > 64 && q + 1 < S.ns ? __ldg(&S.src[q + 1]) : 0;
+    }
+    template <int PI> FFG_DEV_INLINE uint32_t residue(const ColSrc &S, uint64_t i, const PrimeDev &P) const {
+        constexpr uint32_t p = kPrimeC[PI];
+        const uint32_t sft = (uint32_t)(((S.off + i) * S.w) & 63);
+        const uint64_t v = (sft ? (lo >> sft) | (hi << (64 - sft)) : lo) & ((1ull << S.w) - 1);
+        uint32_t l = (uint32_t)v;
+        l = min(l, l - p);
+        l = min(l, l - p);
+        return ad<PI>(l, sh<PI>((uint32_t)(v >> 32), make_uint2(P.c32, P.c32s)));
+    }
+};
+
 // The first step of a power-of-two forward column tile, straight from the
 // digits, when only rows below NZ * (its stride) can be nonzero (a product's
 // operands fill at most the lower half of the transform, a short operand much
 // less): the zero slots are neither read nor transformed (dft_dif_nz).
 // Step A (radix 2^MA at stride 2^RN / 2^MA) when MA > 0, else step B (radix
-// 2^MB at stride 32, one block).
-template <int PI, int RN, int NZ>
-FFG_DEV_INLINE void col_fwd2_first(const PrimeDev &P, const ColSrc &S, uint32_t *smem) {
+// 2^MB at stride 32, one block).  The limb words of a thread's next slot are
+// loaded before its current slot is transformed, so each thread keeps two
+// slots' loads in flight: the strided column reads are latency-bound.
+template <int PI, int RN, int NZ, bool W32>
+FFG_DEV_INLINE void col_fwd2_first_w(const PrimeDev &P, const ColSrc &S, uint32_t *smem) {
     using Q = ColGeo<RN>;
-    const uint64_t *src = S.src;
-    const uint64_t ns = S.ns, cs = S.cs, off = S.off;
-    const uint32_t w = S.w, C = S.C, c0 = S.c0, wc = S.wc, wlg = S.wlg, LS = S.LS;
-    if (Q::MA) {
-        const uint2 *tw = P.stw + c_lines.tw_off[(RN - Q::MA) * 6 + Q::MA];
-        const uint32_t slots = wc * Q::SA;
+    constexpr bool A = Q::MA > 0;
+    constexpr int M = A ? Q::MA : Q::MB;
+    constexpr uint32_t RM = 1u << M, STRIDE = A ? Q::SA : 32, DP = A ? Q::SAP : 33;
+    const uint32_t wc = S.wc, wlg = S.wlg;
+    const uint32_t slots = wc * STRIDE;
+    const uint2 *tw = P.stw + c_lines.tw_off[(A ? RN - Q::MA : 5) * 6 + M];
+    auto index = [&](uint32_t sl, uint32_t t) -> uint64_t {
+        return (uint64_t)((sl >> wlg) + STRIDE * t) * S.C + S.c0 + (sl & (wc - 1));
+    };
+    // prefetch while the two slots' words fit the registers (16 words for
+    // 32-bit digits, 4 digits' limb pairs otherwise)
+    constexpr bool PF = W32 ? NZ <= 16 : NZ <= 4;
+    DigitRaw<W32> cur[NZ];
+    if (PF) {
+#pragma unroll
+        for (uint32_t t = 0; t < (uint32_t)NZ; t++) cur[t].fetch(S, index(threadIdx.x, t), threadIdx.x < slots);
+    }
 #pragma unroll 1
-        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
-            const uint32_t c = s & (wc - 1), j = s >> wlg;
-            uint32_t *d = smem + c * LS + j + (j >> 5);
-            uint32_t x[Q::RA];
+    for (uint32_t sl = threadIdx.x; sl < slots; sl += blockDim.x) {
+        DigitRaw<W32> nxt[PF ? NZ : 1];
+        const uint32_t sn = sl + blockDim.x;
+        if (PF) {
 #pragma unroll
-            for (uint32_t t = 0; t < Q::RA; t++) x[t] = t < (uint32_t)NZ ? FFG_COL_DIGIT(j + Q::SA * t) : 0u;
-            dft_dif_nz<PI, Q::MA, NZ>(x);
+            for (uint32_t t = 0; t < (uint32_t)NZ; t++) nxt[t < (PF ? NZ : 1) ? t : 0].fetch(S, index(sn, t), sn < slots);
+        } else {
 #pragma unroll
-            for (uint32_t t = 1; t < Q::RA; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * Q::SA + j]));
-#pragma unroll
-            for (uint32_t t = 0; t < Q::RA; t++) d[t * Q::SAP] = x[t];
+            for (uint32_t t = 0; t < (uint32_t)NZ; t++) cur[t].fetch(S, index(sl, t), true);
         }
-    } else {
-        const uint2 *tw = P.stw + c_lines.tw_off[5 * 6 + Q::MB];
-        const uint32_t slots = wc * 32;
-#pragma unroll 1
-        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
-            const uint32_t c = s & (wc - 1), j = s >> wlg;
-            uint32_t *d = smem + c * LS + j;
-            uint32_t x[Q::RB];
+        const uint32_t c = sl & (wc - 1), j = sl >> wlg;
+        uint32_t x[RM];
 #pragma unroll
-            for (uint32_t t = 0; t < Q::RB; t++) x[t] = t < (uint32_t)NZ ? FFG_COL_DIGIT(j + 32 * t) : 0u;
-            dft_dif_nz<PI, Q::MB, NZ>(x);
+        for (uint32_t t = 0; t < RM; t++) x[t] = t < (uint32_t)NZ ? cur[t < (uint32_t)NZ ? t : 0].template residue<PI>(S, index(sl, t), P) : 0u;
+        dft_dif_nz<PI, M, NZ>(x);
 #pragma unroll
-            for (uint32_t t = 1; t < Q::RB; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * 32 + j]));
+        for (uint32_t t = 1; t < RM; t++) x[t] = sh<PI>(x[t], __ldg(&tw[(t - 1) * STRIDE + j]));
+        uint32_t *d = smem + c * S.LS + j + (A ? (j >> 5) : 0);
 #pragma unroll
-            for (uint32_t t = 0; t < Q::RB; t++) d[33 * t] = x[t];
+        for (uint32_t t = 0; t < RM; t++) d[t * DP] = x[t];
+        if (PF) {
+#pragma unroll
+            for (uint32_t t = 0; t < (uint32_t)NZ; t++) cur[t] = nxt[t < (PF ? NZ : 1) ? t : 0];
         }
     }
+}
+
+template <int PI, int RN, int NZ>
+FFG_DEV_INLINE void col_fwd2_first(const PrimeDev &P, const ColSrc &S, uint32_t *smem) {
+    if (S.w == 32) col_fwd2_first_w<PI, RN, NZ, true>(P, S, smem);
+    else col_fwd2_first_w<PI, RN, NZ, false>(P, S, smem);
 }
 
 // col_fwd2_first for the least power of two NZ covering nzt slots.
