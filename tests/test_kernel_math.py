@@ -245,3 +245,98 @@ def test_pruned_dif_matches_full():
                 for _ in range(20):
                     x = [rng.randrange(p) if t < nz else 0 for t in range(n)]
                     assert _dif(x, p, w32, nz) == _dif(x, p, w32)
+
+
+# ---------------------------------------------------------------- addressing
+# The fixed-shape passes (ffg_rows.cu, ffg_cols.cu) address shared memory
+# with compile-time offsets from per-group bases.  Restated here for every
+# shape they instantiate: each step touches every word of a line exactly
+# once, stays inside its line, and a warp's simultaneous accesses fall in
+# distinct banks.
+
+COL_SHAPES = {6: (0, 1), 7: (0, 2), 8: (0, 3), 9: (0, 4), 10: (2, 3), 11: (3, 3), 12: (4, 3), 13: (4, 4)}
+ROW_SHAPES = {9: (0, 4), 10: (0, 5), 11: (3, 3), 12: (4, 3), 13: (4, 4)}
+
+
+def pad(i):
+    return i + i // 32
+
+
+def col2_stride(R, wc):
+    wl = min(wc, 32)
+    return ((R + R // 32 + 31) & ~31) + 32 // wl
+
+
+def _col_steps(rn, r3):
+    """(positions of each group) for steps A, B, C of one column line."""
+    MA, MB = COL_SHAPES[rn]
+    R, nblk = 1 << rn, 3 if r3 else 1
+    BP = R + R // 32
+    steps = []
+    if MA:
+        SA = R >> MA
+        groups = []
+        for q in range(nblk):
+            for j in range(SA):
+                groups.append([q * BP + j + j // 32 + t * (SA + SA // 32) for t in range(1 << MA)])
+        steps.append(groups)
+    NB = 32 << MB
+    groups = []
+    for b in range(nblk * R // NB):
+        for j in range(32):
+            groups.append([b * (NB + NB // 32) + j + 33 * t for t in range(1 << MB)])
+    steps.append(groups)
+    groups = []
+    for b in range(nblk * R // 32):
+        q, bl = b >> (rn - 5), b & ((R >> 5) - 1)
+        groups.append([q * BP + 33 * bl + t for t in range(32)])
+    steps.append(groups)
+    return steps
+
+
+def test_column_pass_addressing():
+    for rn in COL_SHAPES:
+        for r3 in (False, True):
+            if r3 and rn > 12:
+                continue
+            R = (3 if r3 else 1) << rn
+            want = sorted(pad(i) for i in range(R))
+            for groups in _col_steps(rn, r3):
+                got = sorted(a for g in groups for a in g)
+                assert got == want, (rn, r3)
+            for wc in (8, 16, 32, 64):
+                LS = col2_stride(R, wc)
+                assert LS > pad(R - 1)
+                # step C: lanes = (column s mod wc, group s / wc); same t
+                C = _col_steps(rn, r3)[-1]
+                for w0 in range(0, min(wc * len(C), 256), 32):
+                    banks = set()
+                    for s in range(w0, w0 + 32):
+                        c, b = s % wc, s // wc
+                        if b < len(C):
+                            banks.add((c * LS + C[b][0]) % 32)
+                    assert len(banks) == min(32, wc * len(C) - w0), (rn, r3, wc)
+
+
+def test_row_pass_addressing():
+    for clg, (MA, MB) in ROW_SHAPES.items():
+        C = 1 << clg
+        T = C // 32
+        want = sorted(pad(i) for i in range(C))
+        seen_a = []
+        if MA:
+            SA = C >> MA
+            for tau in range(T):
+                for k in range(32 >> MA):
+                    j = tau + T * k
+                    seen_a += [j + j // 32 + t * (SA + SA // 32) for t in range(1 << MA)]
+            assert sorted(seen_a) == want
+        NB = 32 << MB
+        seen_b = []
+        for tau in range(T):
+            for k in range(32 >> MB):
+                g = tau + T * k
+                b, j = g >> 5, g & 31
+                seen_b += [b * (NB + NB // 32) + j + 33 * t for t in range(1 << MB)]
+        assert sorted(seen_b) == want
+        assert sorted(33 * tau + t for tau in range(T) for t in range(32)) == want
