@@ -54,34 +54,6 @@ __host__ __device__ inline uint32_t col2_stride(uint32_t R, uint32_t wc) {
     return ((R + R / 32 + 31) & ~31u) + 32 / wl;
 }
 
-// Residue mod p of digit i (width w, from coefficient `off` on) of the
-// operand at src (ns limbs, cs coefficients, zero past them).
-template <int PI>
-FFG_DEV_INLINE uint32_t digit_res(const uint64_t *__restrict__ src, uint64_t ns, uint64_t cs, uint64_t off, uint32_t w,
-                                  uint64_t i, const PrimeDev &P) {
-    constexpr uint32_t p = kPrimeC[PI];
-    if (i >= cs) return 0;
-    if (w == 32) {
-        const uint64_t q = off + i; // the 32-bit word
-        uint32_t l = (q >> 1) < ns ? __ldg((const uint32_t *)src + q) : 0;
-        l = min(l, l - p);
-        return min(l, l - p);
-    }
-    const uint64_t bit = (off + i) * w, q = bit >> 6;
-    const uint32_t s = (uint32_t)(bit & 63);
-    const uint64_t lo = q < ns ? __ldg(&src[q]) : 0;
-    const uint64_t hi = s + w > 64 && q + 1 < ns ? __ldg(&src[q + 1]) : 0;
-    const uint64_t v = (s ? (lo >> s) | (hi << (64 - s)) : lo) & ((1ull << w) - 1);
-    uint32_t l = (uint32_t)v;
-    l = min(l, l - p);
-    l = min(l, l - p);
-    return ad<PI>(l, sh<PI>((uint32_t)(v >> 32), make_uint2(P.c32, P.c32s)));
-}
-
-
-// The digit of row r, column n2 of the operand's four-step layout.
-#define FFG_COL_DIGIT(r) digit_res<PI>(src, ns, cs, off, w, (uint64_t)(r) * C + c0 + c, P)
-
 // What the first step of a forward column tile reads: the operand's digits.
 struct ColSrc {
     const uint64_t *src;
@@ -188,6 +160,60 @@ FFG_DEV_INLINE void col_fwd2_first(const PrimeDev &P, const ColSrc &S, uint32_t 
     else col_fwd2_first_w<PI, RN, NZ, false>(P, S, smem);
 }
 
+// The radix-3 first step (stride 2^RN) of a forward column tile of 3 2^RN
+// rows, straight from the digits, when only the first NB of its three blocks
+// can hold nonzero rows (NB = 1: y0 = x0, y1 = x0 w^j, y2 = x0 w^2j; NB = 2:
+// x2 = 0), with the next slot's limb words loaded before the current slot is
+// transformed, as col_fwd2_first_w.
+template <int PI, int RN, int NB, bool W32>
+FFG_DEV_INLINE void col_fwd2_first_r3(const PrimeDev &P, const ColSrc &S, uint32_t *smem) {
+    using Q = ColGeo<RN>;
+    constexpr uint32_t p = kPrimeC[PI], BP = Q::R + Q::R / 32;
+    constexpr bool PF = W32 || NB <= 2;
+    const uint32_t wc = S.wc, wlg = S.wlg;
+    const uint32_t slots = wc * Q::R;
+    auto index = [&](uint32_t sl, uint32_t q) -> uint64_t {
+        return (uint64_t)((sl >> wlg) + Q::R * q) * S.C + S.c0 + (sl & (wc - 1));
+    };
+    DigitRaw<W32> cur[NB];
+    if (PF) {
+#pragma unroll
+        for (int q = 0; q < NB; q++) cur[q].fetch(S, index(threadIdx.x, q), threadIdx.x < slots);
+    }
+#pragma unroll 1
+    for (uint32_t sl = threadIdx.x; sl < slots; sl += blockDim.x) {
+        DigitRaw<W32> nxt[PF ? NB : 1];
+        const uint32_t sn = sl + blockDim.x;
+        if (PF) {
+#pragma unroll
+            for (int q = 0; q < NB; q++) nxt[PF ? q : 0].fetch(S, index(sn, q), sn < slots);
+        } else {
+#pragma unroll
+            for (int q = 0; q < NB; q++) cur[q].fetch(S, index(sl, q), true);
+        }
+        const uint32_t c = sl & (wc - 1), j = sl >> wlg;
+        const uint32_t x0 = cur[0].template residue<PI>(S, index(sl, 0), P);
+        const uint32_t x1 = NB > 1 ? cur[NB > 1 ? 1 : 0].template residue<PI>(S, index(sl, 1), P) : 0u;
+        const uint32_t x2 = NB > 2 ? cur[NB > 2 ? 2 : 0].template residue<PI>(S, index(sl, 2), P) : 0u;
+        const uint4 t = __ldg(&P.r3f[Q::R + j]);
+        uint32_t *d = smem + c * S.LS + j + (j >> 5);
+        if (NB == 1) {
+            d[0] = x0;
+            d[BP] = sh<PI>(x0, make_uint2(t.x, t.y));
+            d[2 * BP] = sh<PI>(x0, make_uint2(t.z, t.w));
+        } else {
+            const uint32_t u = sh<PI>(x1 - x2 + p, c_lines.w3[PI]);
+            d[0] = ad<PI>(ad<PI>(x0, x1), x2);
+            d[BP] = sh<PI>(ad<PI>(sb<PI>(x0, x2), u), make_uint2(t.x, t.y));
+            d[2 * BP] = sh<PI>(sb<PI>(sb<PI>(x0, x1), u), make_uint2(t.z, t.w));
+        }
+        if (PF) {
+#pragma unroll
+            for (int q = 0; q < NB; q++) cur[q] = nxt[PF ? q : 0];
+        }
+    }
+}
+
 // col_fwd2_first for the least power of two NZ covering nzt slots.
 template <int PI, int RN>
 FFG_DEV_INLINE void col_fwd2_first_any(const PrimeDev &P, const ColSrc &S, uint32_t *smem, uint32_t nzt) {
@@ -212,27 +238,25 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
     const uint64_t ns = op ? J.nb : J.na, cs = op ? J.cb : J.ca, off = op ? J.off_b : J.off_a;
     const uint32_t w = J.width;
 
+    // rows at or past rows_nz are zero in every column of the tile
+    const uint64_t avail = (ns * 64 + w - 1) / w; // digits that start inside the limbs
+    const uint64_t lim = cs < (avail > off ? avail - off : 0) ? cs : (avail > off ? avail - off : 0);
+    const uint64_t rows_nz = lim > c0 ? (lim - c0 + C - 1) / C : 0;
     if (R3) { // radix 3 at stride 2^RN, straight from the digits
-        constexpr uint32_t p = kPrimeC[PI];
-        const uint32_t slots = wc * Q::R;
-#pragma unroll 1
-        for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
-            const uint32_t c = s & (wc - 1), j = s >> wlg;
-            const uint32_t x0 = FFG_COL_DIGIT(j), x1 = FFG_COL_DIGIT(j + Q::R), x2 = FFG_COL_DIGIT(j + 2 * Q::R);
-            const uint4 t = __ldg(&P.r3f[Q::R + j]);
-            const uint32_t u = sh<PI>(x1 - x2 + p, c_lines.w3[PI]);
-            uint32_t *d = smem + c * LS + j + (j >> 5);
-            d[0] = ad<PI>(ad<PI>(x0, x1), x2);
-            d[BP] = sh<PI>(ad<PI>(sb<PI>(x0, x2), u), make_uint2(t.x, t.y));
-            d[2 * BP] = sh<PI>(sb<PI>(sb<PI>(x0, x1), u), make_uint2(t.z, t.w));
+        const ColSrc S{src, ns, cs, off, w, C, c0, wc, wlg, LS};
+        const uint32_t nb = rows_nz <= Q::R ? 1 : rows_nz <= 2 * Q::R ? 2 : 3;
+        if (w == 32) {
+            if (nb == 1) col_fwd2_first_r3<PI, RN, 1, true>(P, S, smem);
+            else if (nb == 2) col_fwd2_first_r3<PI, RN, 2, true>(P, S, smem);
+            else col_fwd2_first_r3<PI, RN, 3, true>(P, S, smem);
+        } else {
+            if (nb == 1) col_fwd2_first_r3<PI, RN, 1, false>(P, S, smem);
+            else if (nb == 2) col_fwd2_first_r3<PI, RN, 2, false>(P, S, smem);
+            else col_fwd2_first_r3<PI, RN, 3, false>(P, S, smem);
         }
         __syncthreads();
     }
     if (!R3) {
-        // rows at or past rows_nz are zero in every column of the tile
-        const uint64_t avail = (ns * 64 + w - 1) / w; // digits that start inside the limbs
-        const uint64_t lim = cs < (avail > off ? avail - off : 0) ? cs : (avail > off ? avail - off : 0);
-        const uint64_t rows_nz = lim > c0 ? (lim - c0 + C - 1) / C : 0;
         const uint32_t stride = Q::MA ? Q::SA : 32;
         const uint32_t nzt = (uint32_t)((rows_nz + stride - 1) / stride);
         const ColSrc S{src, ns, cs, off, w, C, c0, wc, wlg, LS};
@@ -303,10 +327,9 @@ FFG_DEV_INLINE void col_fwd2_body(const PrimeDev &P, const FourStep &G, const FS
         }
     }
 }
-#undef FFG_COL_DIGIT
 
 template <int RN, bool R3>
-__global__ void __launch_bounds__(kLineThreads, R3 ? 2 : 3) k_col_fwd2(Primes3 P3, FourStep G, FSJobs jobs) {
+__global__ void __launch_bounds__(kLineThreads, 3) k_col_fwd2(Primes3 P3, FourStep G, FSJobs jobs) {
     extern __shared__ uint32_t smem[];
     __shared__ FSJob J;
     if (threadIdx.x == 0) {
