@@ -16,7 +16,9 @@ def test_committed_tuning_file_parses(ff):
             continue
         if w[0] == "geometry":
             lg, r3, c, wc = map(int, w[1:])
-            assert 12 <= lg <= 25 and r3 in (0, 1) and 4 <= c <= 13 and wc in (8, 16, 32, 64)
+            # the tuner covers lengths from 2^10; a four-step geometry needs
+            # row lengths 2^4..2^13 and columns of at least 4 words
+            assert 10 <= lg <= 25 and r3 in (0, 1) and 4 <= c <= 13 and lg - c >= 2 and wc in (8, 16, 32, 64)
             rows += 1
         else:
             assert w[0] == "mlp" and int(w[1]) == ff.MLP_NPARAM
