@@ -83,6 +83,11 @@ def lib() -> ctypes.CDLL:
     L.ffg_mul_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64,
                                  ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int,
                                  ctypes.c_void_p]
+    L.ffg_mul_residues.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64,
+                                   ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int,
+                                   ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]
+    L.ffg_crt_residues.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64,
+                                   ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]
     L.ffg_fib_chain.argtypes = [ctypes.c_uint64, ctypes.c_int, _u64p, ctypes.c_size_t, _u64p,
                                 ctypes.c_size_t, ctypes.POINTER(_u64p), _szp]
     L.ffg_last_chain_ms.restype = ctypes.c_double
@@ -529,6 +534,22 @@ def mul_device(out_ptr: int, a_ptr: int, na: int, bits_a: int, b_ptr: int, nb: i
     """ffg_mul_device on device pointers (e.g. torch tensors' data_ptr())."""
     _check(lib().ffg_mul_device(out_ptr, a_ptr, na, bits_a, b_ptr if not square else a_ptr, nb, bits_b,
                                 int(square), stream or None))
+
+
+def mul_residues(y_ptr: int, a_ptr: int, na: int, bits_a: int, b_ptr: int, nb: int, bits_b: int,
+                 square: bool, prime0: int, nprimes: int, stream: int = 0) -> None:
+    """ffg_mul_residues: the scaled convolution of a*b modulo primes
+    [prime0, prime0 + nprimes) into y (3 * plan.L uint32 words, prime-major,
+    device memory); one product's share on a GPU that shards it by prime."""
+    _check(lib().ffg_mul_residues(y_ptr, a_ptr, na, bits_a, b_ptr if not square else a_ptr, nb, bits_b,
+                                  int(square), prime0, nprimes, stream or None))
+
+
+def crt_residues(out_ptr: int, y_ptr: int, na: int, bits_a: int, nb: int, bits_b: int, square: bool,
+                 stream: int = 0) -> None:
+    """ffg_crt_residues: the product (na + nb + 1 limbs into out) from the
+    three primes' residues in y, as gathered from the GPUs that shared it."""
+    _check(lib().ffg_crt_residues(out_ptr, y_ptr, na, bits_a, nb, bits_b, int(square), stream or None))
 
 
 def fib_chain(n: int, i0: int, fkm1, fk) -> np.ndarray:

@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kLineThreads, 3) k_col_fwd2(Primes3 P3, FourSt
         J = jobs.ext ? jobs.ext[i] : jobs.j[i < FFG_FS_JOBS ? i : 0];
     }
     __syncthreads();
-    switch (blockIdx.y) {
+    switch (blockIdx.y + G.prime0) {
     case 0: col_fwd2_body<0, RN, R3>(P3.pr[0], G, J, smem); break;
     case 1: col_fwd2_body<1, RN, R3>(P3.pr[1], G, J, smem); break;
     default: col_fwd2_body<2, RN, R3>(P3.pr[2], G, J, smem); break;
@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(kLineThreads, R3 ? 2 : 3) k_col_inv2(Primes3 P
     __shared__ FSJob J;
     if (threadIdx.x == 0) J = jobs.ext ? jobs.ext[blockIdx.z] : jobs.j[blockIdx.z < FFG_FS_JOBS ? blockIdx.z : 0];
     __syncthreads();
-    switch (blockIdx.y) {
+    switch (blockIdx.y + G.prime0) {
     case 0: col_inv2_body<0, RN, R3>(P3.pr[0], G, J, smem); break;
     case 1: col_inv2_body<1, RN, R3>(P3.pr[1], G, J, smem); break;
     default: col_inv2_body<2, RN, R3>(P3.pr[2], G, J, smem); break;
@@ -485,7 +485,7 @@ static cudaError_t launch_col2_t(bool fwd, const Primes3 &P3, const FourStep &G,
         if (e) return e;
         attr[fwd] = true;
     }
-    const dim3 grid((1u << G.c) / G.wc, 3, nz);
+    const dim3 grid((1u << G.c) / G.wc, G.nprimes, nz);
     // threads per CTA: about one per four groups of the radix-32 step (short
     // columns give a tile few groups; idle threads would only wait)
     const uint32_t groups = G.wc * (uint32_t)(G.R / 32);

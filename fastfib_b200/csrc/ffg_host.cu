@@ -1235,6 +1235,89 @@ extern "C" void ffg_shutdown(void) {
     for (auto &a : g_noalloc_addr) a = nullptr; // looked up again by the next ffg_init
 }
 
+// ======================================================= prime sharding
+//
+// One product over several GPUs by prime: a rank transforms, multiplies and
+// inverts its primes only (the four-step launches over a range of primes,
+// FourStep::prime0 / nprimes), the ranks exchange their slices of the
+// residues (the caller's all-gather, 4 L bytes a prime), and the CRT runs on
+// the gathered array.  The primes' transforms are independent, so that
+// all-gather is the one exchange.
+
+// The product's plan, when it is one prime sharding takes (a four-step plan).
+static int residue_plan(uint64_t bits_a, uint64_t bits_b, int square, ffg_plan *pl) {
+    int rc = plan_select(bits_a, bits_b, square, pl);
+    if (rc) return rc;
+    if (pl->split) return fail(FFG_E_RANGE, "prime sharding: a split product (past the transform cap)");
+    if (pl->kernel == 0)
+        return fail(FFG_E_RANGE, "prime sharding: length %llu is a one-CTA transform (four-step lengths only)",
+                    (unsigned long long)pl->L);
+    return FFG_OK;
+}
+
+extern "C" int ffg_mul_residues(uint32_t *y, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b,
+                                size_t nb, uint64_t bits_b, int square, uint32_t prime0, uint32_t nprimes,
+                                void *stream) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!y || !a || (!square && !b) || na == 0 || (!square && nb == 0) || bits_a == 0 || (!square && bits_b == 0))
+        return fail(FFG_E_ARG, "ffg_mul_residues: bad arguments");
+    if (nprimes == 0 || prime0 >= 3 || nprimes > 3 - prime0)
+        return fail(FFG_E_ARG, "ffg_mul_residues: primes [%u, %u + %u) outside [0, 3)", prime0, prime0, nprimes);
+    if (square) b = a, nb = na, bits_b = bits_a;
+    ffg_plan pl;
+    if ((rc = residue_plan(bits_a, bits_b, square, &pl))) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+    arena_reset();
+    const uint64_t L = pl.L;
+    const uint32_t w = pl.width;
+    FourStep G = four_step_geometry(pl, square != 0);
+    G.prime0 = prime0;
+    G.nprimes = nprimes;
+    FSJobs jobs{};
+    FSJob &J = jobs.j[0];
+    J.a = a, J.b = b, J.na = na, J.nb = nb;
+    J.ca = (bits_a + w - 1) / w;
+    J.cb = (bits_b + w - 1) / w;
+    J.ya = y;
+    J.yb = square ? nullptr : (uint32_t *)arena_alloc(3 * L * sizeof(uint32_t));
+    if (!square && !J.yb) return fail(FFG_E_NOMEM, "device arena: residues of L=%llu", (unsigned long long)L);
+    J.width = w;
+    cudaError_t e = launch_four_step(g.P3, G, jobs, 1, st, 8.0 * (double)(na + (square ? 0 : nb)));
+    if (e) return fail(FFG_E_CUDA, "ffg_mul_residues: %s", cudaGetErrorString(e));
+    return FFG_OK;
+}
+
+extern "C" int ffg_crt_residues(uint64_t *out, const uint32_t *y, size_t na, uint64_t bits_a, size_t nb,
+                                uint64_t bits_b, int square, void *stream) {
+    std::lock_guard<std::recursive_mutex> lk(g_mu);
+    int rc = ensure_ready();
+    if (rc) return rc;
+    if (!out || !y || na == 0 || (!square && nb == 0) || bits_a == 0 || (!square && bits_b == 0))
+        return fail(FFG_E_ARG, "ffg_crt_residues: bad arguments");
+    if (square) nb = na, bits_b = bits_a;
+    ffg_plan pl;
+    if ((rc = residue_plan(bits_a, bits_b, square, &pl))) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+    arena_reset();
+    const uint32_t w = pl.width;
+    CrtJob C{};
+    C.y = y;
+    C.y_stride = pl.L;
+    C.conv = (bits_a + w - 1) / w + (bits_b + w - 1) / w - 1;
+    C.out = out;
+    C.nlimbs = na + nb + 1;
+    C.width = w;
+    C.add = 0;
+    C.maps = (uint32_t *)arena_alloc((size_t)crt_ctas(C.nlimbs, w) * sizeof(uint32_t));
+    if (!C.maps) return fail(FFG_E_NOMEM, "device arena: CRT scratch");
+    C.ticket = ticket_get();
+    cudaError_t e = launch_crt(g.P3, C, st);
+    if (e) return fail(FFG_E_CUDA, "ffg_crt_residues: %s", cudaGetErrorString(e));
+    return FFG_OK;
+}
+
 // ======================================================= allocation-free multiply
 //
 // ffg_mul_device_noalloc: the NTT product of ffg_mul_device for callers that

@@ -48,6 +48,9 @@ struct FourStep {
     uint32_t mode;          // RowMode of k_row_conv
     uint64_t mstep;         // M / L
     uint32_t scl[3], scls[3];
+    // the launch's primes: [prime0, prime0 + nprimes) (blockIdx.y counts
+    // from prime0); all three but for a product sharded by prime
+    uint32_t prime0 = 0, nprimes = 3;
 };
 
 // One product of a four-step launch.  ya / yb: 3 * L words each (prime-major);

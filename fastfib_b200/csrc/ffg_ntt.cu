@@ -43,10 +43,10 @@ FFG_DEV_INLINE void job_to_smem(const L &list, uint32_t i, T *dst) {
 
 cudaError_t set_line_consts(const LineConsts &h) { return cudaMemcpyToSymbol(c_lines, &h, sizeof h); }
 
-// Calls body<PI>(...) for the CTA's prime (blockIdx.y), so each prime's
-// constants are compile-time inside the body.
-#define FFG_PRIME_DISPATCH(body, ...)                                                                  \
-    switch (blockIdx.y) {                                                                            \
+// Calls body<PI>(...) for the CTA's prime (blockIdx.y, counted from first),
+// so each prime's constants are compile-time inside the body.
+#define FFG_PRIME_DISPATCH_FROM(first, body, ...)                                                      \
+    switch (blockIdx.y + (first)) {                                                                  \
     case 0: body<0>(P3.pr[0], __VA_ARGS__); break;                                                   \
     case 1: body<1>(P3.pr[1], __VA_ARGS__); break;                                                   \
     default: body<2>(P3.pr[2], __VA_ARGS__); break;                                                  \
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kLineThreads, kLineMinBlocks) k_conv_small(Pri
     __shared__ ConvJob J;
     job_to_smem<ConvJobs, ConvJob, FFG_CONV_JOBS>(jobs, blockIdx.x, &J);
     __syncthreads();
-    FFG_PRIME_DISPATCH(conv_small_body, J, smem)
+    FFG_PRIME_DISPATCH_FROM(0, conv_small_body, J, smem)
 }
 
 // ------------------------------------------------------------- four-step
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(kLineThreads, kLineMinBlocks) k_col_fwd(Primes
     __shared__ FSJob J;
     job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, G.square ? blockIdx.z : (blockIdx.z >> 1), &J);
     __syncthreads();
-    FFG_PRIME_DISPATCH(col_fwd_body, G, J, smem)
+    FFG_PRIME_DISPATCH_FROM(G.prime0, col_fwd_body, G, J, smem)
 }
 
 // One row (position pos of the column transform) per CTA.  ROW_CONV: forward
@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(kLineThreads, kLineMinBlocks) k_row_conv(Prime
     __shared__ FSJob J;
     job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, blockIdx.z, &J);
     __syncthreads();
-    FFG_PRIME_DISPATCH(row_body, G, J, smem)
+    FFG_PRIME_DISPATCH_FROM(G.prime0, row_body, G, J, smem)
 }
 
 template <int PI>
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(kLineThreads, kLineMinBlocks) k_col_inv(Primes
     __shared__ FSJob J;
     job_to_smem<FSJobs, FSJob, FFG_FS_JOBS>(jobs, blockIdx.z, &J);
     __syncthreads();
-    FFG_PRIME_DISPATCH(col_inv_body, G, J, smem)
+    FFG_PRIME_DISPATCH_FROM(G.prime0, col_inv_body, G, J, smem)
 }
 
 // ---------------------------------------------------------------- launchers
@@ -310,7 +310,7 @@ cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs 
     if (col2) {
         e = launch_col2(true, P3, G, jobs, njobs * nops, st);
     } else {
-        k_col_fwd<<<dim3(tiles, 3, njobs * nops), 256, sm_col, st>>>(P3, G, jobs);
+        k_col_fwd<<<dim3(tiles, G.nprimes, njobs * nops), 256, sm_col, st>>>(P3, G, jobs);
         e = cudaGetLastError();
     }
     prof_end(PK_COL_FWD, st, res * nops + limb_bytes);
@@ -319,7 +319,7 @@ cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs 
     if (g_row2 && row2_ok(G)) {
         e = launch_row2(P3, G, jobs, njobs, st);
     } else {
-        k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, jobs);
+        k_row_conv<<<dim3(G.R, G.nprimes, njobs), 256, sm_row, st>>>(P3, G, jobs);
         e = cudaGetLastError();
     }
     prof_end(PK_ROW_CONV, st, res * (nops + 1));
@@ -328,7 +328,7 @@ cudaError_t launch_four_step(const Primes3 &P3, const FourStep &G, const FSJobs 
     if (col2) {
         e = launch_col2(false, P3, G, jobs, njobs, st);
     } else {
-        k_col_inv<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, jobs);
+        k_col_inv<<<dim3(tiles, G.nprimes, njobs), 256, sm_col, st>>>(P3, G, jobs);
         e = cudaGetLastError();
     }
     prof_end(PK_COL_INV, st, res * 2);
@@ -357,13 +357,13 @@ cudaError_t launch_split_forward(const Primes3 &P3, FourStep G, const FSJobs &jo
     if (g_col2 && col2_ok(G)) {
         e = launch_col2(true, P3, G, jobs, njobs, st);
     } else {
-        k_col_fwd<<<dim3(tiles, 3, njobs), 256, sm_col, st>>>(P3, G, jobs);
+        k_col_fwd<<<dim3(tiles, G.nprimes, njobs), 256, sm_col, st>>>(P3, G, jobs);
         e = cudaGetLastError();
     }
     prof_end(PK_COL_FWD, st, res + limb_bytes);
     if (e) return e;
     prof_begin(PK_ROW_CONV, st);
-    k_row_conv<<<dim3(G.R, 3, njobs), 256, sm_row, st>>>(P3, G, jobs);
+    k_row_conv<<<dim3(G.R, G.nprimes, njobs), 256, sm_row, st>>>(P3, G, jobs);
     prof_end(PK_ROW_CONV, st, res * 2);
     return cudaGetLastError();
 }
@@ -381,14 +381,14 @@ cudaError_t launch_split_piece(const Primes3 &P3, FourStep G, const FSJob &job, 
     const uint32_t tiles = (1u << G.c) / G.wc;
     const double res = 3.0 * 4.0 * (double)G.L;
     prof_begin(PK_ROW_CONV, st);
-    k_row_conv<<<dim3(G.R, 3, 1), 256, sm_row, st>>>(P3, G, one);
+    k_row_conv<<<dim3(G.R, G.nprimes, 1), 256, sm_row, st>>>(P3, G, one);
     prof_end(PK_ROW_CONV, st, res * (2.0 * pairs + 1.0));
     if ((e = cudaGetLastError())) return e;
     prof_begin(PK_COL_INV, st);
     if (g_col2 && col2_ok(G)) {
         e = launch_col2(false, P3, G, one, 1, st);
     } else {
-        k_col_inv<<<dim3(tiles, 3, 1), 256, sm_col, st>>>(P3, G, one);
+        k_col_inv<<<dim3(tiles, G.nprimes, 1), 256, sm_col, st>>>(P3, G, one);
         e = cudaGetLastError();
     }
     prof_end(PK_COL_INV, st, res * 3.0);

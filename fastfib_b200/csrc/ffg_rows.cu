@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256, (CLG == 10 && !SQ) ? 2 : 3) k_row2(Primes
     __shared__ FSJob J;
     if (threadIdx.x == 0) J = jobs.ext ? jobs.ext[blockIdx.z] : jobs.j[blockIdx.z < FFG_FS_JOBS ? blockIdx.z : 0];
     __syncthreads();
-    switch (blockIdx.y) {
+    switch (blockIdx.y + G.prime0) {
     case 0: row2_body<0, CLG, SQ>(P3.pr[0], G, J, smem); break;
     case 1: row2_body<1, CLG, SQ>(P3.pr[1], G, J, smem); break;
     default: row2_body<2, CLG, SQ>(P3.pr[2], G, J, smem); break;
@@ -264,10 +264,10 @@ static cudaError_t launch_row2_t(const Primes3 &P3, const FourStep &G, const FSJ
     // rows per CTA: as many as fit 256 threads, halved while the launch would
     // have fewer than three CTAs per SM (short rows of a mid-size product)
     uint32_t rows = Q::ROWS;
-    while (rows > 1 && (uint64_t)(G.R / rows) * 3 * njobs < 3 * 148) rows >>= 1;
+    while (rows > 1 && (uint64_t)(G.R / rows) * G.nprimes * njobs < 3 * 148) rows >>= 1;
     while (rows > 1 && G.R % rows) rows >>= 1;
     const size_t sm = (size_t)rows * (SQ ? 1 : 2) * Q::LS * sizeof(uint32_t);
-    k_row2<CLG, SQ><<<dim3(G.R / rows, 3, njobs), rows * Q::T, sm, st>>>(P3, G, jobs);
+    k_row2<CLG, SQ><<<dim3(G.R / rows, G.nprimes, njobs), rows * Q::T, sm, st>>>(P3, G, jobs);
     return cudaGetLastError();
 }
 

@@ -12,6 +12,13 @@ the products are gathered afterwards -- the only collective is that gather.
 a cost estimate per product: for an NTT product the transform length L of the
 library's own plan (ffg_plan_select) times log2 L, for a product small enough
 for schoolbook na * nb limb products scaled to the same units.
+
+One product too large for one GPU's time budget shards by prime instead
+(``mul_prime_sharded``): the three primes' transforms, pointwise products and
+inverses are independent (src/mul_ntt.c:29-48 runs them one after another),
+so each rank runs its primes' share (ffg_mul_residues), one broadcast per
+prime from its owner completes every rank's residues -- 4 L bytes a prime,
+the only exchange -- and the CRT (ffg_crt_residues) recombines them.
 """
 from __future__ import annotations
 
@@ -123,3 +130,103 @@ def mul_batch_sharded(pairs, method: str = "plain", group=None, dst: int = 0, mu
     got = mul([pairs[i] for i in share]) if share else []
     local = {i: np.asarray(g, dtype=np.uint64) for i, g in zip(share, got)}
     return gather_products(local, len(pairs), group=group, dst=dst), share
+
+
+def prime_shares(world: int) -> list[tuple[int, int]]:
+    """(prime0, nprimes) of every rank when one product's three primes are
+    spread over `world` ranks: contiguous ranges as even as three allows
+    (two ranks: one prime and two); ranks past the third get (0, 0)."""
+    used = min(world, 3)
+    out = []
+    for r in range(world):
+        if r >= used:
+            out.append((0, 0))
+        else:
+            lo, hi = 3 * r // used, 3 * (r + 1) // used
+            out.append((lo, hi - lo))
+    return out
+
+
+def _bits(x: np.ndarray) -> int:
+    nz = np.flatnonzero(x)
+    if nz.size == 0:
+        return 0
+    top = int(nz[-1])
+    return 64 * top + int(x[top]).bit_length()
+
+
+def mul_prime_sharded(a, b=None, group=None, dst=None, residues=None, crt=None, plan=None):
+    """The product a * b (b None: a squared) with its three primes spread over
+    the ranks of group (prime_shares).  Each rank computes its primes'
+    residues, one broadcast per prime from the rank that owns it fills in the
+    others, and the CRT recombines all three on rank dst (every rank when dst
+    is None); other ranks return None.  The product is returned as limbs.
+
+    By default the work runs on this rank's GPU through the library
+    (ffg_mul_residues / ffg_crt_residues) and the residues stay in device
+    memory for the broadcasts (NCCL).  The tests pass the oracle's instead:
+    residues(a, b, square, k) -> prime k's L words, crt(y (3 x L), a, b,
+    square) -> limbs, and plan(bits_a, bits_b, square) -> {"L", "width",
+    "kernel", "split"}; the buffers then live on the CPU (gloo)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    square = b is None
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    b = a if square else np.ascontiguousarray(b, dtype=np.uint64)
+    bits_a, bits_b = _bits(a), _bits(b)
+    if bits_a == 0 or bits_b == 0:
+        raise ValueError("mul_prime_sharded: a zero factor")
+    library = residues is None
+    if plan is None:
+        import fastfib_b200 as ff
+        plan = ff.plan
+    pl = plan(bits_a, bits_b, square)
+    if pl["split"] or not pl["kernel"]:
+        raise ValueError("mul_prime_sharded: four-step plans only (not a one-CTA length or a split product)")
+    L = int(pl["L"])
+    prime0, nprimes = prime_shares(world)[rank]
+    shares = prime_shares(world)
+    if not library:
+        y = torch.zeros((3, L), dtype=torch.int32)
+        for k in range(prime0, prime0 + nprimes):
+            y[k] = torch.from_numpy(np.asarray(residues(a, b, square, k), dtype=np.uint32).view(np.int32))
+        _broadcast_primes(y, shares, group)
+        if dst is not None and rank != dst:
+            return None
+        return np.asarray(crt(y.numpy().view(np.uint32), a, b, square), dtype=np.uint64)
+    import fastfib_b200 as ff
+    dev = torch.device("cuda", torch.cuda.current_device())
+    # a stream of our own: the library runs on the stream it is given (NULL,
+    # the legacy default stream's handle, would mean its own stream), and the
+    # uploads, the broadcasts (NCCL waits on the current stream) and the CRT
+    # must all be ordered on it
+    side = torch.cuda.Stream(device=dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        stream = side.cuda_stream
+        da = torch.from_numpy(a.view(np.int64)).to(dev)
+        db = da if square else torch.from_numpy(b.view(np.int64)).to(dev)
+        y = torch.zeros((3, L), dtype=torch.int32, device=dev)
+        if nprimes:
+            ff.mul_residues(y.data_ptr(), da.data_ptr(), a.size, bits_a, db.data_ptr(), b.size, bits_b, square,
+                            prime0, nprimes, stream)
+        _broadcast_primes(y, shares, group)
+        if dst is not None and rank != dst:
+            side.synchronize()
+            return None
+        out = torch.empty(a.size + b.size + 1, dtype=torch.int64, device=dev)
+        ff.crt_residues(out.data_ptr(), y.data_ptr(), a.size, bits_a, b.size, bits_b, square, stream)
+        res = out.cpu().numpy().view(np.uint64)
+    return res
+
+
+def _broadcast_primes(y, shares, group):
+    """Every prime's row of y from the rank that owns it; every rank takes the
+    same three broadcasts, in order."""
+    import torch.distributed as dist
+    for k in range(3):
+        owner = next(r for r, (p0, n) in enumerate(shares) if p0 <= k < p0 + n)
+        src = dist.get_global_rank(group, owner) if group is not None else owner
+        dist.broadcast(y[k], src=src, group=group)

@@ -223,6 +223,23 @@ int ffg_load_tuning(const char *path);
 int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b,
                            size_t nb, uint64_t bits_b, int square, void *stream);
 
+/* One product sharded over GPUs by prime (one process per GPU; no counterpart
+   in the reference, whose three primes run on one host, src/mul_ntt.c:97-118).
+   ffg_mul_residues runs the forward transforms, the pointwise product and the
+   inverse of primes [prime0, prime0 + nprimes) only, for the plan
+   ffg_plan_select gives (four-step plans only: FFG_E_RANGE for a one-CTA
+   length or a split product).  y: 3 * plan.L words of device memory,
+   prime-major; prime k's scaled convolution lands in y[k L .. k L + conv),
+   the other primes' words are left as they are.  The caller exchanges the
+   slices (an all-gather of 4 L bytes per prime), then ffg_crt_residues
+   recombines all three primes of y into out (na + nb + 1 limbs of device
+   memory, fully written), exactly the product ffg_mul_device writes.
+   Arguments as for ffg_mul_device; stream: a cudaStream_t or NULL. */
+int ffg_mul_residues(uint32_t *y, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b, size_t nb,
+                     uint64_t bits_b, int square, uint32_t prime0, uint32_t nprimes, void *stream);
+int ffg_crt_residues(uint64_t *out, const uint32_t *y, size_t na, uint64_t bits_a, size_t nb, uint64_t bits_b,
+                     int square, void *stream);
+
 /* fibonacci (src/fib.c:211) from bit i0 down: continues fast doubling from
    the pair (F(k-1), F(k)), k = n >> i0, on the device and returns F(n) as a
    limb array in pinned host memory (free with ffg_free).  i0 >= 1. */

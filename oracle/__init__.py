@@ -197,6 +197,29 @@ class Oracle(_Lib):
         ptr = self.lib.fo_mul_ntt_forced(pa, na, pb, nb, int(square), width, L, ctypes.byref(n))
         return self._take(ptr, n.value)
 
+    def residues(self, a, b, width: int, L: int, k: int, square=False) -> np.ndarray:
+        """Prime k's scaled convolution of a * b at (width, L): L uint32 words."""
+        a, pa, na = _arr(a)
+        b, pb, nb = (a, pa, na) if square else _arr(b)
+        y = np.zeros(L, dtype=np.uint32)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        self.lib.fo_residues.argtypes = [_u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, ctypes.c_int,
+                                         ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, u32p]
+        if self.lib.fo_residues(pa, na, pb, nb, int(square), width, L, k, y.ctypes.data_as(u32p)):
+            raise ValueError(f"residues: L={L} too short, or prime {k} / width {width} out of range")
+        return y
+
+    def crt_residues(self, y: np.ndarray, L: int, conv: int, width: int, limbs: int) -> np.ndarray:
+        """The product from all three primes' residues (y: 3 x L uint32)."""
+        y = np.ascontiguousarray(y, dtype=np.uint32).reshape(-1)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        self.lib.fo_crt_residues.restype = ctypes.c_void_p
+        self.lib.fo_crt_residues.argtypes = [u32p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                                             ctypes.c_size_t, _szp]
+        n = ctypes.c_size_t()
+        ptr = self.lib.fo_crt_residues(y.ctypes.data_as(u32p), L, conv, width, limbs, ctypes.byref(n))
+        return self._take(ptr, n.value)
+
     def fingerprint(self, a) -> tuple:
         a, pa, na = _arr(a)
         out = (ctypes.c_uint64 * 6)()

@@ -452,27 +452,32 @@ static Num crt_pack(uint32_t *const y[3], uint64_t conv, unsigned b, size_t limb
     return (Num){d, nlen(d, limbs)};
 }
 
+/* One prime's cyclic convolution of the width-w digits of a and b at length
+   L, scaled by 1/L (src/mul_ntt.c:29-48): L words, malloc'd. */
+static uint32_t *conv_prime(const Num *a, const Num *b, int square, unsigned w, uint64_t L, int k) {
+    uint64_t ca = (num_bits(a) + w - 1) / w, cb = (num_bits(b) + w - 1) / w;
+    uint32_t p = P[k];
+    uint32_t *fa = xcal(L, 4), *fb = square ? fa : xcal(L, 4);
+    for (uint64_t i = 0; i < ca; i++) fa[i] = (uint32_t)(digit(a, i, w) % p);
+    if (!square)
+        for (uint64_t i = 0; i < cb; i++) fb[i] = (uint32_t)(digit(b, i, w) % p);
+    dft(fa, L, 0, p, G[k]);
+    if (!square) dft(fb, L, 0, p, G[k]);
+    for (uint64_t i = 0; i < L; i++) fa[i] = mm(fa[i], fb[i], p);
+    dft(fa, L, 1, p, G[k]);
+    uint32_t linv = pw((uint32_t)(L % p), p - 2, p);
+    for (uint64_t i = 0; i < L; i++) fa[i] = mm(fa[i], linv, p);
+    if (!square) free(fb);
+    return fa;
+}
+
 /* big_mul_ntt for a given width and transform length: three cyclic
-   convolutions (src/mul_ntt.c:29-48), then the CRT (src/mul_ntt.c:65-73). */
+   convolutions, then the CRT (src/mul_ntt.c:65-73). */
 static Num mul_ntt_plain(const Num *a, const Num *b, int square, unsigned w, uint64_t L) {
     size_t bits_a = num_bits(a), bits_b = num_bits(b);
     uint64_t ca = (bits_a + w - 1) / w, cb = (bits_b + w - 1) / w, conv = ca + cb - 1;
     uint32_t *y[3];
-    for (int k = 0; k < 3; k++) {
-        uint32_t p = P[k];
-        uint32_t *fa = xcal(L, 4), *fb = square ? fa : xcal(L, 4);
-        for (uint64_t i = 0; i < ca; i++) fa[i] = (uint32_t)(digit(a, i, w) % p);
-        if (!square)
-            for (uint64_t i = 0; i < cb; i++) fb[i] = (uint32_t)(digit(b, i, w) % p);
-        dft(fa, L, 0, p, G[k]);
-        if (!square) dft(fb, L, 0, p, G[k]);
-        for (uint64_t i = 0; i < L; i++) fa[i] = mm(fa[i], fb[i], p);
-        dft(fa, L, 1, p, G[k]);
-        uint32_t linv = pw((uint32_t)(L % p), p - 2, p);
-        for (uint64_t i = 0; i < L; i++) fa[i] = mm(fa[i], linv, p);
-        if (!square) free(fb);
-        y[k] = fa;
-    }
+    for (int k = 0; k < 3; k++) y[k] = conv_prime(a, b, square, w, L, k);
     Num r = crt_pack(y, conv, w, a->n + b->n + 1);
     for (int k = 0; k < 3; k++) free(y[k]);
     return r;
@@ -942,6 +947,35 @@ uint64_t *fo_mul_ntt_forced(const uint64_t *a, size_t na, const uint64_t *b, siz
     Num r = (num_is_zero(&A) || num_is_zero(&B)) ? num_u64(0) : mul_ntt_plain(&A, &B, square, width, L);
     num_free(&A);
     if (!square) num_free(&B);
+    return take(&r, nout);
+}
+
+/* One prime's share of a product sharded by prime: the scaled convolution
+   modulo prime k (0..2) at width and length L into y[0 .. L); -1 when L does
+   not hold the product's coefficients. */
+int fo_residues(const uint64_t *a, size_t na, const uint64_t *b, size_t nb, int square, uint32_t width,
+                uint64_t L, int k, uint32_t *y) {
+    Num A = num_copy_raw(a, na), B = square ? A : num_copy_raw(b, nb);
+    const uint64_t ca = (num_bits(&A) + width - 1) / width, cb = (num_bits(&B) + width - 1) / width;
+    if (k < 0 || k > 2 || width < 1 || width > 35 || ca + cb - 1 > L) {
+        num_free(&A);
+        if (!square) num_free(&B);
+        return -1;
+    }
+    uint32_t *f = conv_prime(&A, &B, square, width, L, k);
+    memcpy(y, f, L * 4);
+    free(f);
+    num_free(&A);
+    if (!square) num_free(&B);
+    return 0;
+}
+
+/* The product from all three primes' residues (y: 3 * L words, prime-major),
+   conv coefficients of width bits, limbs limbs at most. */
+uint64_t *fo_crt_residues(const uint32_t *y, uint64_t L, uint64_t conv, uint32_t width, size_t limbs,
+                          size_t *nout) {
+    uint32_t *const ys[3] = {(uint32_t *)y, (uint32_t *)y + L, (uint32_t *)y + 2 * L};
+    Num r = crt_pack(ys, conv, width, limbs);
     return take(&r, nout);
 }
 

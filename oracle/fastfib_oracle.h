@@ -45,6 +45,13 @@ uint64_t *fo_mul(const uint64_t *a, size_t na, const uint64_t *b, size_t nb, int
 uint64_t *fo_mul_ntt(const uint64_t *a, size_t na, const uint64_t *b, size_t nb, int square, size_t *nout);
 uint64_t *fo_mul_ntt_forced(const uint64_t *a, size_t na, const uint64_t *b, size_t nb, int square,
                             uint32_t width, uint64_t L, size_t *nout);
+/* A product sharded by prime: prime k's scaled convolution at (width, L)
+   into y[0 .. L) (-1 when L is too short); the product from all three
+   primes' residues (3 L words). */
+int fo_residues(const uint64_t *a, size_t na, const uint64_t *b, size_t nb, int square, uint32_t width,
+                uint64_t L, int k, uint32_t *y);
+uint64_t *fo_crt_residues(const uint32_t *y, uint64_t L, uint64_t conv, uint32_t width, size_t limbs,
+                          size_t *nout);
 uint64_t *fo_fibonacci(uint64_t n, size_t *nout);
 char *fo_to_string(const uint64_t *a, size_t na);
 void fo_fingerprint(const uint64_t *a, size_t na, uint64_t out[6]);

@@ -88,7 +88,10 @@ def test_device_batch(ff):
         jobs.append({"a": ta.data_ptr(), "b": None if sq else tb.data_ptr(), "na": a.size,
                      "nb": a.size if sq else b.size, "bits_a": 64 * a.size, "bits_b": 64 * (a.size if sq else b.size),
                      "out": out.data_ptr(), "square": sq, "method": ("plain", "ntt", "school")[i % 3]})
-    ff.mul_batch_device(jobs, torch.cuda.current_stream().cuda_stream)
+    # on a stream of our own, after the uploads (NULL would be the library's stream)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    ff.mul_batch_device(jobs, side.cuda_stream)
     torch.cuda.synchronize()
     for i, ((a, b), j) in enumerate(zip(pairs, jobs)):
         out = keep[3 * i + 2].cpu().numpy().view(np.uint64)

@@ -1,7 +1,9 @@
-"""CPU tests of the by-product sharding (fastfib_b200/shard.py): the cost
-partition of the uneven product stream over 2..8 ranks, and the sharded
-batch with its gather on two gloo ranks, each rank's share computed by the
-oracle, whose union on rank 0 must be exactly the single-rank result."""
+"""CPU tests of the sharding over GPUs (fastfib_b200/shard.py): the cost
+partition of the uneven product stream over 2..8 ranks; the sharded batch
+with its gather on two gloo ranks, each rank's share computed by the oracle,
+whose union on rank 0 must be exactly the single-rank result; and one product
+sharded by prime over two and three gloo ranks, each rank computing only its
+primes' residues (the oracle's), the product recombined on every rank."""
 import os
 import socket
 
@@ -103,3 +105,78 @@ def test_sharded_batch_on_two_gloo_ranks():
         res[r] = (ok, n)
     assert res[0][0] is True and res[1][0] is True
     assert res[0][1] + res[1][1] == len(_pairs()) and res[0][1] > 0 and res[1][1] > 0
+
+
+def test_prime_shares():
+    from fastfib_b200.shard import prime_shares
+    assert prime_shares(1) == [(0, 3)]
+    assert prime_shares(2) == [(0, 1), (1, 2)]
+    assert prime_shares(3) == [(0, 1), (1, 1), (2, 1)]
+    assert prime_shares(5)[3:] == [(0, 0), (0, 0)]
+    for w in range(1, 9):  # every prime owned by exactly one rank
+        owned = [k for p0, n in prime_shares(w) for k in range(p0, p0 + n)]
+        assert sorted(owned) == [0, 1, 2]
+
+
+def _prime_rank(rank, world, port, q):
+    import sys
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from fastfib_b200.shard import _bits, mul_prime_sharded, prime_shares
+        from oracle import Oracle, int_to_limbs, limbs_to_int
+        o = Oracle()
+        o.ntt_init(1 << 16)
+        rng = np.random.default_rng(21)
+        cases = [(rng.integers(0, 2**63, 3000, dtype=np.uint64), rng.integers(0, 2**63, 2100, dtype=np.uint64)),
+                 (rng.integers(0, 2**63, 2600, dtype=np.uint64), None),
+                 (int_to_limbs((1 << (64 * 1500)) - 1), int_to_limbs((1 << (64 * 1700)) - 1))]
+        calls = []
+
+        def plan(bits_a, bits_b, square):
+            p = o.plan(bits_a, bits_b, square)
+            return {"L": p.L, "width": p.width, "split": p.split, "kernel": 1}
+
+        def residues(a, b, square, k):
+            calls.append(k)
+            p = o.plan(_bits(a), _bits(b), square)
+            return o.residues(a, b, p.width, p.L, k, square)
+
+        def crt(y, a, b, square):
+            p = o.plan(_bits(a), _bits(b), square)
+            ca = (_bits(a) + p.width - 1) // p.width
+            cb = (_bits(b) + p.width - 1) // p.width
+            return o.crt_residues(y, p.L, ca + cb - 1, p.width, a.size + b.size + 1)
+
+        ok = True
+        for a, b in cases:
+            got = mul_prime_sharded(a, b, residues=residues, crt=crt, plan=plan)
+            want = limbs_to_int(a) * limbs_to_int(a if b is None else b)
+            ok = ok and limbs_to_int(got) == want
+        p0, n = prime_shares(world)[rank]
+        mine = sorted(set(calls)) == list(range(p0, p0 + n)) and len(calls) == n * len(cases)
+        dist.barrier()
+        q.put((rank, ok, mine))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_prime_sharded_product_on_gloo_ranks(world):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_prime_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    res = {}
+    for _ in range(world):
+        r, ok, mine = q.get(timeout=10)
+        res[r] = (ok, mine)
+    assert all(ok and mine for ok, mine in res.values()), res
