@@ -244,6 +244,46 @@ static const size_t kBatchSmallMin = 64;       // products of one plan (a decima
 // group of products sharing an NTT plan one transform launch set and one CRT
 // launch; split products one by one.  Job records go to the device in one
 // copy.
+// Streams a batch's plan groups run on besides the caller's (its lanes), with
+// the events that fork them from and join them back to the caller's stream.
+// FFG_BATCH_LANES sets the number of lanes, the caller's stream included
+// (default 4; 1 runs every group on the caller's stream).
+constexpr int kMaxLanes = 8;
+static cudaStream_t g_lane[kMaxLanes - 1];
+static cudaEvent_t g_fork = nullptr, g_join[kMaxLanes - 1];
+static int g_lanes_made = 0;
+
+static int batch_lanes() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("FFG_BATCH_LANES");
+        v = e && *e ? atoi(e) : 4;
+        v = std::max(1, std::min(kMaxLanes, v));
+    }
+    return v;
+}
+
+// Side streams 1 .. n - 1 and their events, made once (before any capture).
+static cudaError_t lanes_make(int n) {
+    cudaError_t e = cudaSuccess;
+    if (!g_fork && (e = cudaEventCreateWithFlags(&g_fork, cudaEventDisableTiming))) return e;
+    for (; g_lanes_made < n - 1; g_lanes_made++) {
+        if ((e = cudaStreamCreateWithFlags(&g_lane[g_lanes_made], cudaStreamNonBlocking))) return e;
+        if ((e = cudaEventCreateWithFlags(&g_join[g_lanes_made], cudaEventDisableTiming))) return e;
+    }
+    return e;
+}
+
+void lanes_free() {
+    for (int i = 0; i < g_lanes_made; i++) {
+        cudaStreamDestroy(g_lane[i]);
+        cudaEventDestroy(g_join[i]);
+    }
+    g_lanes_made = 0;
+    if (g_fork) cudaEventDestroy(g_fork);
+    g_fork = nullptr;
+}
+
 int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capture) {
     // Many products of one four-step plan up to L = kBatchSmallMaxL: one CTA
     // per (product, prime) holding the whole transform beats three launches
@@ -359,6 +399,31 @@ int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capture) {
         if (!dimg) return fail(FFG_E_NOMEM, "device arena: batch job records");
         CK(cudaMemcpyAsync(dimg, img.data(), img.size(), cudaMemcpyHostToDevice, st));
     }
+    // The plan groups are independent until the CRTs: they run on lanes (the
+    // caller's stream and side streams forked from it, joined back before the
+    // CRT launch), so the launches of small groups, which leave most SMs idle,
+    // overlap the large ones.  Groups go to the least loaded lane, largest
+    // predicted cost first (count x L log L; the schoolbook launch by its
+    // limb products).
+    const int nlanes = std::min<int>(batch_lanes(), (int)launches.size() + (sj.empty() ? 0 : 1));
+    std::vector<int> lane_of(launches.size(), 0);
+    int school_lane = 0;
+    if (nlanes > 1) {
+        CK(lanes_make(nlanes));
+        std::vector<std::pair<double, int>> order; // (cost, index; -1 the schoolbook launch)
+        for (size_t i = 0; i < launches.size(); i++)
+            order.push_back({(double)launches[i].count * (double)launches[i].pl.L * (launches[i].pl.lg + 2), (int)i});
+        if (!sj.empty()) order.push_back({school_bytes * school_bytes / (64.0 * (double)sj.size()), -1});
+        std::sort(order.begin(), order.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+        std::vector<double> load(nlanes, 0.0);
+        for (const auto &o : order) {
+            const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            load[l] += o.first;
+            if (o.second < 0) school_lane = l;
+            else lane_of[o.second] = l;
+        }
+    }
+    auto lane = [&](int l) { return l == 0 ? st : g_lane[l - 1]; };
     // with `capture`, the launches (not the job upload) become a CUDA graph
     // instead of running: the autotuner replays it to time the device alone
     if (capture) {
@@ -367,7 +432,19 @@ int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capture) {
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         g_capturing = true;
     }
+    bool forked = false;
+    auto join = [&]() -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        for (int l = 1; forked && l < nlanes && !e; l++) {
+            e = cudaEventRecord(g_join[l - 1], lane(l));
+            if (!e) e = cudaStreamWaitEvent(st, g_join[l - 1], 0);
+        }
+        forked = false;
+        return e;
+    };
     auto end_capture = [&](int rc) -> int {
+        cudaError_t je = join();
+        if (!rc && je) rc = fail(FFG_E_CUDA, "batch lanes: %s", cudaGetErrorString(je));
         if (!capture) return rc;
         g_capturing = false;
         cudaGraph_t gr = nullptr;
@@ -381,18 +458,26 @@ int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capture) {
         return FFG_OK;
     };
     cudaError_t e;
+    if (nlanes > 1) {
+        forked = true;
+        e = cudaEventRecord(g_fork, st);
+        for (int l = 1; l < nlanes && !e; l++) e = cudaStreamWaitEvent(lane(l), g_fork, 0);
+        if (e) return end_capture(fail(FFG_E_CUDA, "batch lanes: %s", cudaGetErrorString(e)));
+    }
     for (size_t base = 0; base < sj.size(); base += 65535) {
         const uint32_t cnt = (uint32_t)std::min<size_t>(65535, sj.size() - base);
-        e = launch_school_batch((const SchoolJob *)(dimg + school_off) + base, cnt, school_ctas_max, st,
-                                school_bytes * cnt / sj.size());
+        e = launch_school_batch((const SchoolJob *)(dimg + school_off) + base, cnt, school_ctas_max,
+                                lane(school_lane), school_bytes * cnt / sj.size());
         if (e) return end_capture(fail(FFG_E_CUDA, "schoolbook batch: %s", cudaGetErrorString(e)));
     }
-    for (const Launch &ln : launches) {
+    for (size_t li = 0; li < launches.size(); li++) {
+        const Launch &ln = launches[li];
+        const cudaStream_t ls = lane(lane_of[li]);
         const bool sq = ln.key.square != 0;
         if (ln.key.kernel == 0) {
             ConvJobs cjs{};
             cjs.ext = (const ConvJob *)(dimg + ln.conv_off);
-            e = launch_conv_small(g.P3, cjs, (uint32_t)ln.count, (uint32_t)ln.pl.L, !sq, st, ln.conv_bytes);
+            e = launch_conv_small(g.P3, cjs, (uint32_t)ln.count, (uint32_t)ln.pl.L, !sq, ls, ln.conv_bytes);
             if (e) return end_capture(fail(FFG_E_CUDA, "batched one-CTA transforms: %s", cudaGetErrorString(e)));
         } else {
             FourStep G = four_step_geometry(ln.pl, sq);
@@ -401,11 +486,12 @@ int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capture) {
                 FSJobs fjs{};
                 fjs.ext = (const FSJob *)(dimg + ln.conv_off) + base;
                 const uint32_t cnt = (uint32_t)std::min(per, ln.count - base);
-                e = launch_four_step(g.P3, G, fjs, cnt, st, ln.conv_bytes * cnt / ln.count);
+                e = launch_four_step(g.P3, G, fjs, cnt, ls, ln.conv_bytes * cnt / ln.count);
                 if (e) return end_capture(fail(FFG_E_CUDA, "batched four-step: %s", cudaGetErrorString(e)));
             }
         }
     }
+    if ((e = join())) return end_capture(fail(FFG_E_CUDA, "batch lanes: %s", cudaGetErrorString(e)));
     if (!crts.empty()) {
         e = launch_crt_flat((const CrtJob *)(dimg + crt_off), (const uint32_t *)(dimg + first_off),
                             (uint32_t)crts.size(), crt_first.back(), st, crt_bytes);

@@ -1223,6 +1223,7 @@ extern "C" void ffg_shutdown(void) {
     cudaFree(g.tables);
     g.tables = nullptr;
     mlp_free();
+    lanes_free();
     if (g_tickets) cudaFree(g_tickets);
     g_tickets = nullptr;
     dec_free();

@@ -123,6 +123,8 @@ int method_plan(int method, uint64_t bits_a, uint64_t bits_b, int square, BJob *
 int run_batch(std::vector<BJob> &jobs, cudaStream_t st, cudaGraph_t *capture = nullptr);
 // Frees the cost model's device parameters.
 void mlp_free();
+// Destroys the batches' side streams and their events.
+void lanes_free();
 
 // ---------------------------------------------------------------- decimal
 
