@@ -32,6 +32,9 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC = os.path.join(ROOT, "profiles", "roofline_traffic.json")
 METRIC = "F(n) ms at n=1e8/1e9 on 1 B200, bit-exact; learned vs plain; NTT % HBM peak"
 PUBLISHED_F1E8_MS = 46.0  # the reference's README, F(10^8) on an i9-9900K
+# how oracle/_ref is compiled (oracle/Makefile): the reference's own sources,
+# unmodified; it asks for -march=native, the AVX2 level it needs is x86-64-v3
+REF_BUILD = "gcc -O3 -march=x86-64-v3 from the reference's sources (it asks for -march=native)"
 FALLBACK_HBM_GBS = 6650.0  # an earlier copy-bandwidth measurement on B200
 
 
@@ -135,6 +138,8 @@ def cpu_baseline(n, steps=7):
     out = {"value": best * 1e3, "unit": "ms", "cores": cores, "kind": kind,
            "sample": f"F({n}) best of {steps} runs after one warm-up, all pool threads"}
     if kind == "reference":
+        out["build"] = REF_BUILD
+    if kind == "reference":
         f = run(n)
         dec = float("inf")
         for _ in range(3):
@@ -170,7 +175,8 @@ def run_reference(args, rank, world):
     base.update({"value": v, "ms_per_step": v, "scaling": "weak", "vs_baseline": v / PUBLISHED_F1E8_MS
                  if args.n == 10**8 else None,
                  "cpu_baseline": {"value": v, "unit": "ms", "cores": cores, "kind": kind,
-                                  "sample": f"F({args.n}) x {args.steps} after {args.warmup} warm-ups"},
+                                  "sample": f"F({args.n}) x {args.steps} after {args.warmup} warm-ups",
+                                  **({"build": REF_BUILD} if kind == "reference" else {})},
                  "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                  "bit_exact": ok})
     print(json.dumps(base), flush=True)
