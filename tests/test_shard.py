@@ -180,3 +180,42 @@ def test_prime_sharded_product_on_gloo_ranks(world):
         r, ok, mine = q.get(timeout=10)
         res[r] = (ok, mine)
     assert all(ok and mine for ok, mine in res.values()), res
+
+
+def test_prime_sharded_one_rank_and_refusals(oracle):
+    """One gloo rank computes all three primes itself; plans prime sharding
+    does not take (a one-CTA length, a split product) and zero factors are
+    refused before any collective."""
+    import torch.distributed as dist
+    from fastfib_b200.shard import _bits, mul_prime_sharded
+    from oracle import limbs_to_int
+    oracle.ntt_init(1 << 16)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(_free_port()))
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        def plan(bits_a, bits_b, square, kernel=1, split=None):
+            p = oracle.plan(bits_a, bits_b, square)
+            return {"L": p.L, "width": p.width, "split": p.split if split is None else split, "kernel": kernel}
+
+        def residues(a, b, square, k):
+            p = oracle.plan(_bits(a), _bits(b), square)
+            return oracle.residues(a, b, p.width, p.L, k, square)
+
+        def crt(y, a, b, square):
+            p = oracle.plan(_bits(a), _bits(b), square)
+            conv = (_bits(a) + p.width - 1) // p.width + (_bits(b) + p.width - 1) // p.width - 1
+            return oracle.crt_residues(y, p.L, conv, p.width, a.size + b.size + 1)
+
+        rng = np.random.default_rng(3)
+        a = rng.integers(0, 2**64, 1500, dtype=np.uint64)
+        b = rng.integers(0, 2**64, 1100, dtype=np.uint64)
+        got = mul_prime_sharded(a, b, residues=residues, crt=crt, plan=plan)
+        assert limbs_to_int(got) == limbs_to_int(a) * limbs_to_int(b)
+        with pytest.raises(ValueError):  # a one-CTA length
+            mul_prime_sharded(a, b, residues=residues, crt=crt, plan=lambda *x: plan(*x, kernel=0))
+        with pytest.raises(ValueError):  # a split product
+            mul_prime_sharded(a, b, residues=residues, crt=crt, plan=lambda *x: plan(*x, split=1))
+        with pytest.raises(ValueError):  # a zero factor
+            mul_prime_sharded(np.zeros(4, np.uint64), b, residues=residues, crt=crt, plan=plan)
+    finally:
+        dist.destroy_process_group()
