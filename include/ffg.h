@@ -68,7 +68,9 @@ int ffg_mul_host(uint64_t *out, size_t *nout, const uint64_t *a, size_t na, cons
                  int square);
 /* big_mul_ntt on device limbs.  bits_a / bits_b: bit lengths (upper bounds
    are allowed; leading zero limbs are fine).  out: na + nb + 1 limbs of
-   device memory, fully written.  stream: a cudaStream_t or NULL. */
+   device memory, fully written.  stream: a cudaStream_t, or NULL for the
+   library's own stream (non-blocking: not ordered after work on the legacy
+   default stream). */
 int ffg_mul_device(uint64_t *out, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b, size_t nb,
                    uint64_t bits_b, int square, void *stream);
 
@@ -234,7 +236,7 @@ int ffg_mul_device_noalloc(uint64_t *out, const uint64_t *a, size_t na, uint64_t
    slices (an all-gather of 4 L bytes per prime), then ffg_crt_residues
    recombines all three primes of y into out (na + nb + 1 limbs of device
    memory, fully written), exactly the product ffg_mul_device writes.
-   Arguments as for ffg_mul_device; stream: a cudaStream_t or NULL. */
+   Arguments and stream as for ffg_mul_device. */
 int ffg_mul_residues(uint32_t *y, const uint64_t *a, size_t na, uint64_t bits_a, const uint64_t *b, size_t nb,
                      uint64_t bits_b, int square, uint32_t prime0, uint32_t nprimes, void *stream);
 int ffg_crt_residues(uint64_t *out, const uint32_t *y, size_t na, uint64_t bits_a, size_t nb, uint64_t bits_b,
