@@ -69,8 +69,10 @@ def test_learned_is_bit_exact(ff):
 
 def test_trained_model_gain(ff):
     """Plain thresholds against the trained cost model on the uneven stream
-    (1024 products, 2^10..2^24 bits, aspect up to 16): the learned batch must
-    not be slower, and the test prints the gain."""
+    (1024 products, 2^10..2^24 bits, aspect up to 16), device times of graph
+    replays: the learned batch must not be slower than the plain one beyond
+    0.5 % (the replays' timing noise; the measured gain is 1-2 %), and the test
+    prints the gain."""
     torch = pytest.importorskip("torch")
     if not ff.load_tuning():
         pytest.skip("no trained cost model (run python -m fastfib_b200.tune on a GPU)")
@@ -89,4 +91,4 @@ def test_trained_model_gain(ff):
         t[m] = ff.time_batch([dict(j, method=m) for j in base], reps=3)
     print(f"uneven stream, 1024 products: plain {t['plain']:.3f} ms, learned {t['learned']:.3f} ms, "
           f"gain {t['plain'] / t['learned']:.2f}x")
-    assert t["learned"] <= 1.05 * t["plain"]
+    assert t["learned"] <= 1.005 * t["plain"]
