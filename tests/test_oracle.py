@@ -180,3 +180,34 @@ def test_split_tiny_caps(oracle, lg):
             assert limbs_to_int(oracle.mul_ntt(int_to_limbs(x))) == x * x, (lg, na)
     finally:
         oracle.set_ntt_max_L(saved)
+
+
+@pytest.mark.parametrize("square", [False, True])
+def test_residues_are_the_digit_convolution(oracle, square):
+    """One prime's share of a prime-sharded product (fo_residues) is the plain
+    convolution of the operands' width-w digits modulo that prime, word for
+    word, zero past the product's coefficients; the three shares' CRT
+    (fo_crt_residues) is the product."""
+    P = (2113929217, 2013265921, 1811939329)
+    rng = np.random.default_rng(11)
+    a = rng.integers(0, 2**64, 37, dtype=np.uint64)
+    b = a if square else rng.integers(0, 2**64, 29, dtype=np.uint64)
+    x, y = limbs_to_int(a), limbs_to_int(b)
+    for w, L in ((32, 256), (35, 192)):
+        ca, cb = -(-x.bit_length() // w), -(-y.bit_length() // w)
+        da = [(x >> (w * i)) & ((1 << w) - 1) for i in range(ca)]
+        db = [(y >> (w * i)) & ((1 << w) - 1) for i in range(cb)]
+        conv = [0] * (ca + cb - 1)
+        for i, u in enumerate(da):
+            for j, v in enumerate(db):
+                conv[i + j] += u * v
+        ys = []
+        for k, p in enumerate(P):
+            got = oracle.residues(a, b, w, L, k, square)
+            assert [int(v) for v in got[:len(conv)]] == [c % p for c in conv], (w, k)
+            assert not got[len(conv):].any()
+            ys.append(got)
+        prod = oracle.crt_residues(np.stack(ys), L, len(conv), w, a.size + b.size + 1)
+        assert limbs_to_int(prod) == x * y
+    with pytest.raises(ValueError):  # a length that does not hold the product
+        oracle.residues(a, b, 32, 64, 0, square)
